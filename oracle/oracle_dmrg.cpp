@@ -1,0 +1,967 @@
+// Oracle DMRG: Lanczos (eigen.f90), density matrix + truncation (den_mat.f90),
+// operator enlargement and U^dagger O U (block.f90:2495-3683, get_sys.f90:4-1055),
+// wave transformations and sweep drivers (dmrg_sub.f90:974-1789, main.f90:114-209).
+// TEST INFRASTRUCTURE ONLY (see oracle.hpp).
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <stdexcept>
+
+#include "oracle.hpp"
+
+extern "C" {
+void scipy_zheev_(const char*, const char*, const int*, void*, const int*, double*, void*,
+                  const int*, double*, int*);
+void scipy_dstev_(const char*, const int*, double*, double*, double*, const int*, double*, int*);
+}
+
+namespace orc {
+
+namespace {
+const cplx cone(1.0, 0.0), czero(0.0, 0.0);
+inline int find_bs(const Basis& b, int up, int down) {
+  for (int x = 0; x < b.num; ++x)
+    if (b.sub[x].new_num_up == up && b.sub[x].new_num_down == down) return x;
+  return -1;
+}
+inline int find_blk(const Block& b, int up, int down) {
+  for (int k = 0; k < b.num; ++k)
+    if (b.sub[k].num_up == up && b.sub[k].num_down == down) return k;
+  return -1;
+}
+inline int find_blk3(const Block& b, int up, int down, int dd) {
+  for (int k = 0; k < b.num; ++k)
+    if (b.sub[k].num_up == up && b.sub[k].num_down == down && b.sub[k].down_dif == dd) return k;
+  return -1;
+}
+inline double pm1(int e) { return ((e % 2) + 2) % 2 == 0 ? 1.0 : -1.0; }
+
+// dstev wrapper; d/e overwritten; z (n x n) when jobz=='V'
+void dstev(char jobz, int n, std::vector<double>& d, std::vector<double>& e, std::vector<double>* z) {
+  if (n <= 0) return;
+  std::vector<double> work(std::max(1, 2 * n - 2));
+  std::vector<double> zz;
+  int ldz = n, info = 0;
+  if (jobz == 'V') zz.assign((size_t)n * n, 0.0);
+  else zz.assign(1, 0.0);
+  scipy_dstev_(&jobz, &n, d.data(), e.data(), zz.data(), &ldz, work.data(), &info);
+  if (z) *z = zz;
+}
+
+// update_block_dia, block.f90:2495-2548
+void update_block_dia(const Block& block, const Basis& basis, Block& nb) {
+  nb = Block();
+  nb.len = basis.len;
+  nb.num = basis.num;
+  nb.dim = basis.dim;
+  nb.sub.assign(nb.num, SubBlock());
+  for (int i = 0; i < nb.num; ++i) {
+    SubBlock& s = nb.sub[i];
+    s.num_up = basis.sub[i].new_num_up;
+    s.num_down = basis.sub[i].new_num_down;
+    s.down_dif = 0;
+    s.row_dim = s.sdim = basis.sub[i].dim;
+    s.mat.assign((size_t)s.sdim * s.sdim, 0.0);
+  }
+  for (int k = 0; k < nb.num; ++k)
+    for (const auto& p : basis.sub[k].sub) {
+      for (int i = 0; i < block.num; ++i) {
+        const SubBlock& b = block.sub[i];
+        if (b.num_up == p.bl_num_up && b.num_down == p.bl_num_down) {
+          double c1 = std::sqrt((1.0 + nb.sub[k].num_down) / (1.0 + b.num_down));
+          for (int c = 0; c < p.sdim; ++c)
+            for (int r = 0; r < p.sdim; ++r) nb.sub[k].at(p.spos + r, p.spos + c) += b.at(r, c) * c1;
+          break;
+        }
+      }
+    }
+}
+
+// update_site_dia, block.f90:2554-2615
+void update_site_dia(const Block& site, const Basis& basis, Block& ns) {
+  ns = Block();
+  ns.len = basis.len;
+  ns.num = basis.num;
+  ns.dim = basis.dim;
+  ns.sub.assign(ns.num, SubBlock());
+  for (int i = 0; i < ns.num; ++i) {
+    SubBlock& s = ns.sub[i];
+    s.num_up = basis.sub[i].new_num_up;
+    s.num_down = basis.sub[i].new_num_down;
+    s.down_dif = 0;
+    s.row_dim = s.sdim = basis.sub[i].dim;
+    s.mat.assign((size_t)s.sdim * s.sdim, 0.0);
+  }
+  for (int k = 0; k < ns.num; ++k)
+    for (const auto& p : basis.sub[k].sub) {
+      for (int i = 0; i < site.num; ++i) {
+        const SubBlock& st = site.sub[i];
+        if (st.num_up == p.st_num_up && st.num_down == p.st_num_down) {
+          double c1 = std::sqrt((1.0 + ns.sub[k].num_down) / (1.0 + st.num_down));
+          for (int y = 0; y < p.sdim; ++y) ns.sub[k].at(p.spos + y, p.spos + y) += st.mat[0] * c1;
+          break;
+        }
+      }
+    }
+}
+
+// sub-block structure shared by update_*_ndia_* (block.f90:2655-2712)
+void ndia_structure(const Basis& basis, int up_dif, int K, Block& nb) {
+  nb.sub.clear();
+  nb.dim = 0;
+  for (int x = 0; x < basis.num; ++x)
+    for (int dd = -K; dd <= K; dd += 2) {
+      int lu = basis.sub[x].new_num_up + up_dif, ld = basis.sub[x].new_num_down + dd;
+      int y = find_bs(basis, lu, ld);
+      if (y < 0) continue;
+      SubBlock s;
+      s.num_up = basis.sub[x].new_num_up;
+      s.num_down = basis.sub[x].new_num_down;
+      s.down_dif = dd;
+      s.row_dim = basis.sub[y].dim;
+      s.sdim = basis.sub[x].dim;
+      s.mat.assign((size_t)s.row_dim * s.sdim, 0.0);
+      nb.dim += s.sdim;
+      nb.sub.push_back(std::move(s));
+    }
+  nb.num = (int)nb.sub.size();
+}
+
+// update_block_ndia_sys (block.f90:2624-2820) and _env (block.f90:2828-3036)
+void update_block_ndia(const Block& block, const Basis& basis, Block& nb, char FlagSign, bool env) {
+  nb = Block();
+  nb.len = basis.len;
+  nb.up_dif = block.up_dif;
+  nb.down_dif = block.down_dif;
+  int up_dif = block.up_dif, K = block.down_dif;
+  ndia_structure(basis, up_dif, K, nb);
+  for (int i = 0; i < nb.num; ++i) {
+    SubBlock& o = nb.sub[i];
+    int rhs_id = find_bs(basis, o.num_up, o.num_down);
+    int lhs_id = find_bs(basis, o.num_up + up_dif, o.num_down + o.down_dif);
+    if (rhs_id < 0 || lhs_id < 0) continue;
+    int lhs_num_down = o.num_down + o.down_dif, rhs_num_down = o.num_down;
+    for (const auto& p : basis.sub[rhs_id].sub) {
+      for (int sdd = -K; sdd <= K; sdd += 2) {
+        int bid = find_blk3(block, p.bl_num_up, p.bl_num_down, sdd);
+        if (bid < 0) continue;
+        int lsu = p.bl_num_up + up_dif, lsd = p.bl_num_down + sdd;
+        const SubBasisMap* q = nullptr;
+        for (const auto& qq : basis.sub[lhs_id].sub)
+          if (qq.bl_num_up == lsu && qq.bl_num_down == lsd && qq.st_num_down == p.st_num_down) {
+            q = &qq;
+            break;
+          }
+        if (!q) continue;
+        double Signs = 1.0;
+        if (env && FlagSign == 'F') Signs = (p.st_num_up % 2 == 0) ? 1.0 : -1.0;
+        int j1 = lhs_num_down, j2 = K, j3 = rhs_num_down, j4 = p.bl_num_down, j5 = p.st_num_down, j6 = lsd;
+        double coef = w6js(j1, j2, j3, j4, j5, j6);
+        if (!env) {
+          coef = coef * std::sqrt((1.0 + j1) * (1.0 + j3));
+          coef = coef * pm1((j6 + j5 + j3 + j2) / 2);
+        } else {
+          coef = coef * pm1((j6 + j5 + j3 + j2) / 2) * std::sqrt((1.0 + j1) * (1.0 + j3));
+        }
+        if (coef == 0.0) continue;
+        coef = coef * Signs;
+        const SubBlock& b = block.sub[bid];
+        for (int c = 0; c < p.sdim; ++c)
+          for (int r = 0; r < q->sdim; ++r) o.at(q->spos + r, p.spos + c) += coef * b.at(r, c);
+      }
+    }
+  }
+}
+
+// update_site_ndia_sys (block.f90:3047-3260) and _env (block.f90:3269-3459)
+void update_site_ndia(const Block& site, const Basis& basis, Block& ns, char FlagSign, bool env) {
+  ns = Block();
+  ns.len = basis.len;
+  ns.up_dif = site.up_dif;
+  ns.down_dif = site.down_dif;
+  int up_dif = site.up_dif, K = site.down_dif;
+  ndia_structure(basis, up_dif, K, ns);
+  for (int i = 0; i < ns.num; ++i) {
+    SubBlock& o = ns.sub[i];
+    int rhs_id = find_bs(basis, o.num_up, o.num_down);
+    int lhs_id = find_bs(basis, o.num_up + up_dif, o.num_down + o.down_dif);
+    if (rhs_id < 0 || lhs_id < 0) continue;
+    int lhs_num_down = o.num_down + o.down_dif, rhs_num_down = o.num_down;
+    for (const auto& p : basis.sub[rhs_id].sub) {
+      for (int sdd = -K; sdd <= K; sdd += 2) {
+        int sid = find_blk3(site, p.st_num_up, p.st_num_down, sdd);
+        if (sid < 0) continue;
+        int lsu = p.st_num_up + up_dif, lsd = p.st_num_down + sdd;
+        const SubBasisMap* q = nullptr;
+        for (const auto& qq : basis.sub[lhs_id].sub)
+          if (qq.st_num_up == lsu && qq.st_num_down == lsd && qq.bl_num_down == p.bl_num_down) {
+            q = &qq;
+            break;
+          }
+        if (!q) continue;
+        double Signs = 1.0;
+        if (!env && FlagSign == 'F') Signs = (p.bl_num_up % 2 == 0) ? 1.0 : -1.0;
+        int j1 = lhs_num_down, j2 = K, j3 = rhs_num_down, j4 = p.st_num_down, j5 = p.bl_num_down, j6 = lsd;
+        double coef = w6js(j1, j2, j3, j4, j5, j6);
+        if (!env) coef = coef * pm1((j5 + j4 + j1 + j2) / 2) * std::sqrt((1.0 + j1) * (1.0 + j3));
+        else coef = coef * std::sqrt((1.0 + j1) * (1.0 + j3)) * pm1((j5 + j4 + j1 + j2) / 2);
+        if (coef == 0.0) continue;
+        coef = coef * Signs;
+        cplx v = site.sub[sid].mat[0];
+        for (int y = 0; y < p.sdim; ++y) o.at(q->spos + y, p.spos + y) += coef * v;
+      }
+    }
+  }
+}
+
+// Get_hamiltonian_dia, get_sys.f90:776-854 (Flag1=Flag2='N', FlagConjg=.false.)
+void hamiltonian_dia(const Block& o1, const Block& o2, cplx coef, Block& ham) {
+  std::vector<cplx> mat;
+  for (int i = 0; i < ham.num; ++i) {
+    SubBlock& h = ham.sub[i];
+    int a = find_blk(o1, h.num_up, h.num_down);
+    int b = find_blk(o2, h.num_up, h.num_down);
+    if (a < 0 || b < 0) continue;
+    int sdim = h.sdim;
+    mat.assign((size_t)sdim * sdim, 0.0);
+    cplx c1 = coef / std::sqrt(1.0 + h.num_down);
+    zgemm('N', 'N', sdim, sdim, sdim, c1, o1.sub[a].mat.data(), sdim, o2.sub[b].mat.data(), sdim,
+          czero, mat.data(), sdim);
+    for (size_t e = 0; e < mat.size(); ++e) h.mat[e] += mat[e];
+  }
+}
+
+// Get_hamiltonian_ndia, get_sys.f90:865-1055
+void hamiltonian_ndia(const Block& block, const Block& site, const Basis& basis, cplx coef,
+                      Block& ham, char FlagSign, char Flags) {
+  int up_dif = block.up_dif, K = block.down_dif;
+  for (int i = 0; i < ham.num; ++i) {
+    SubBlock& h = ham.sub[i];
+    int rhs_id = find_bs(basis, h.num_up, h.num_down);
+    int lhs_id = find_bs(basis, h.num_up, h.num_down + h.down_dif);
+    if (rhs_id < 0 || lhs_id < 0) continue;
+    int rhs_num_down = h.num_down;
+    for (const auto& p : basis.sub[rhs_id].sub) {
+      for (int sdd = -K; sdd <= K; sdd += 2) {
+        int bid = find_blk3(block, p.bl_num_up, p.bl_num_down, sdd);
+        if (bid < 0) continue;
+        int lsu = p.bl_num_up + up_dif, lsd = p.bl_num_down + sdd;
+        for (int nsd = std::abs(p.st_num_down - site.down_dif); nsd <= p.st_num_down + site.down_dif;
+             nsd += 2) {
+          int st_down_dif = p.st_num_down - nsd;
+          int nsu = p.st_num_up - site.up_dif;
+          int sid = find_blk3(site, nsu, nsd, st_down_dif);
+          const SubBasisMap* q = nullptr;
+          for (const auto& qq : basis.sub[lhs_id].sub)
+            if (qq.bl_num_up == lsu && qq.bl_num_down == lsd && qq.st_num_down == nsd) {
+              q = &qq;
+              break;
+            }
+          if (!q || sid < 0) continue;
+          int j1 = lsd, j2 = p.bl_num_down, j3 = K, j4 = p.st_num_down, j5 = nsd, j6 = rhs_num_down;
+          double c11 = w6js(j1, j2, j3, j4, j5, j6);
+          c11 = c11 * std::sqrt((1.0 + j6) / (1.0 + j3)) * pm1((j2 + j5 + j3 + j6) / 2) *
+                site.sub[sid].mat[0].real();
+          cplx smat = site.sub[sid].mat[0];
+          double Sign = 1.0;
+          if (Flags == 'S') {
+            if (FlagSign == 'F' && (p.bl_num_up % 2) == 1) Sign = -1.0;
+          } else {
+            if (FlagSign == 'F' && (p.st_num_up % 2) == 0) Sign = -1.0;
+          }
+          (void)smat;
+          if (c11 == 0.0) continue;
+          cplx c1 = c11 * coef * Sign;
+          const SubBlock& b = block.sub[bid];
+          int ld = q->sdim, rd = p.sdim;
+          for (int c = 0; c < rd; ++c)
+            for (int r = 0; r < ld; ++r) h.at(q->spos + r, p.spos + c) += c1 * b.at(r, c);
+          if (site.up_dif != 0) {
+            cplx cc = std::conj(c1);
+            for (int c = 0; c < ld; ++c)
+              for (int r = 0; r < rd; ++r) h.at(p.spos + r, q->spos + c) += cc * std::conj(b.at(c, r));
+          }
+        }
+      }
+    }
+  }
+}
+
+// update_trun_dia, block.f90:3465-3527
+void update_trun_dia(const Block& ori, Block& eff, const Block& trun) {
+  eff = Block();
+  eff.len = ori.len;
+  eff.num = trun.num;
+  eff.dim = trun.dim;
+  eff.up_dif = ori.up_dif;
+  eff.down_dif = ori.down_dif;
+  eff.sub.assign(eff.num, SubBlock());
+  std::vector<cplx> mid;
+  for (int i = 0; i < eff.num; ++i) {
+    SubBlock& e = eff.sub[i];
+    e.num_up = trun.sub[i].num_up;
+    e.num_down = trun.sub[i].num_down;
+    e.down_dif = 0;
+    e.row_dim = e.sdim = trun.sub[i].sdim;
+    e.mat.assign((size_t)e.sdim * e.sdim, 0.0);
+  }
+  for (int i = 0; i < eff.num; ++i) {
+    SubBlock& e = eff.sub[i];
+    int x = find_blk(ori, e.num_up, e.num_down);
+    if (x < 0) continue;
+    int od = ori.sub[x].row_dim, ed = e.sdim;
+    mid.assign((size_t)od * ed, 0.0);
+    zgemm('N', 'N', od, ed, od, cone, ori.sub[x].mat.data(), od, trun.sub[i].mat.data(), od, czero,
+          mid.data(), od);
+    zgemm('C', 'N', ed, ed, od, cone, trun.sub[i].mat.data(), od, mid.data(), od, czero,
+          e.mat.data(), ed);
+  }
+}
+
+// update_trun_ndia, block.f90:3535-3683
+void update_trun_ndia(const Block& ori, Block& eff, const Block& trun) {
+  eff = Block();
+  eff.len = ori.len;
+  eff.up_dif = ori.up_dif;
+  eff.down_dif = ori.down_dif;
+  int up_dif = ori.up_dif, K = ori.down_dif;
+  for (int x = 0; x < trun.num; ++x)
+    for (int dd = -K; dd <= K; dd += 2) {
+      int y = find_blk(trun, trun.sub[x].num_up + up_dif, trun.sub[x].num_down + dd);
+      if (y < 0) continue;
+      SubBlock s;
+      s.num_up = trun.sub[x].num_up;
+      s.num_down = trun.sub[x].num_down;
+      s.down_dif = dd;
+      s.row_dim = trun.sub[y].sdim;
+      s.sdim = trun.sub[x].sdim;
+      s.mat.assign((size_t)s.row_dim * s.sdim, 0.0);
+      eff.dim += s.sdim;
+      eff.sub.push_back(std::move(s));
+    }
+  eff.num = (int)eff.sub.size();
+  std::vector<cplx> mid;
+  for (int i = 0; i < eff.num; ++i) {
+    SubBlock& e = eff.sub[i];
+    int rhs_id = find_blk(trun, e.num_up, e.num_down);
+    int lhs_id = find_blk(trun, e.num_up + up_dif, e.num_down + e.down_dif);
+    int ori_id = find_blk3(ori, e.num_up, e.num_down, e.down_dif);
+    if (rhs_id < 0 || lhs_id < 0 || ori_id < 0) continue;
+    int orow = ori.sub[ori_id].row_dim, ocol = ori.sub[ori_id].sdim;
+    int rd = trun.sub[rhs_id].sdim, ld = trun.sub[lhs_id].sdim;
+    mid.assign((size_t)orow * rd, 0.0);
+    zgemm('N', 'N', orow, rd, ocol, cone, ori.sub[ori_id].mat.data(), orow,
+          trun.sub[rhs_id].mat.data(), ocol, czero, mid.data(), orow);
+    zgemm('C', 'N', ld, rd, orow, cone, trun.sub[lhs_id].mat.data(), orow, mid.data(), orow, czero,
+          e.mat.data(), ld);
+  }
+}
+
+// QuickSort_Double, block.f90:2398-2444 (descending, carries an index array)
+void quicksort_double(std::vector<double>& arr, std::vector<int>& idx, int lower, int upper) {
+  int i = lower, j = upper;
+  int index = (int)((lower + upper) / 2.0);
+  double mn = arr[index];
+  while (i <= j) {
+    while (arr[i] > mn) i++;
+    while (arr[j] < mn) j--;
+    if (i <= j) {
+      std::swap(arr[i], arr[j]);
+      std::swap(idx[i], idx[j]);
+      i++;
+      j--;
+    }
+  }
+  if (lower < j) quicksort_double(arr, idx, lower, j);
+  if (i < upper) quicksort_double(arr, idx, i, upper);
+}
+
+}  // namespace
+
+// ---- Lanczos (eigen.f90:4-199), levels=1 ------------------------------------------
+void Oracle::lanczos_memo_new(Model& sys, Model& env, const Basis& sys_bs, const Basis& env_bs,
+                              const Super& super, Wave& eigvec, int* iters, double* e0) {
+  const int loop_out = 4, loop_in = 100;
+  int iter_out = 0, last = 1;
+  double lastmin = 1024.0, ritzmin = 0.0;
+  std::vector<double> alpha1(loop_in + 1), beta1(loop_in + 1);
+  std::vector<Wave> t(loop_in + 2);
+  bool done = false;
+  while (iter_out <= loop_out && !done) {
+    iter_out++;
+    last = 1;
+    std::fill(alpha1.begin(), alpha1.end(), 0.0);
+    std::fill(beta1.begin(), beta1.end(), 0.0);
+    ritzmin = lastmin;
+    t[last] = eigvec;
+    wave_normalize(t[last]);
+    allocate_wave(super, t[last + 1]);
+    hmerge(sys, env, sys_bs, env_bs);
+    model_wave(sys, env, sys_bs, env_bs, t[last], t[last + 1]);
+    alpha1[last] = wave_product(t[last], t[last + 1]);
+    ritzmin = alpha1[last];
+    bool converged = false;
+    while (last < loop_in) {
+      Wave& w = t[last + 1];
+      for (int i = 0; i < w.num; ++i) {
+        auto& v = w.sub[i].vec;
+        const auto& a = t[last].sub[i].vec;
+        if (last < 2) {
+          for (size_t e = 0; e < v.size(); ++e) v[e] = v[e] - alpha1[last] * a[e];
+        } else {
+          const auto& b = t[last - 1].sub[i].vec;
+          for (size_t e = 0; e < v.size(); ++e) v[e] = v[e] - alpha1[last] * a[e] - beta1[last - 1] * b[e];
+        }
+      }
+      beta1[last] = wave_norm(w);
+      if (std::fabs(beta1[last]) <= lanzero) {
+        converged = true;
+        break;
+      }
+      wave_normalize(w);
+      // Gram_Schmidt_process (block.f90:1251-1289) against t[1..last]
+      {
+        std::vector<double> uv(last + 1), uu(last + 1);
+        for (int j = 1; j <= last; ++j) {
+          uv[j] = wave_product(t[j], w);
+          uu[j] = wave_product(t[j], t[j]);
+        }
+        Wave tmp = w;
+        for (auto& s : tmp.sub) std::fill(s.vec.begin(), s.vec.end(), czero);
+        for (int j = 1; j <= last; ++j)
+          for (int i = 0; i < tmp.num; ++i) {
+            auto& tv = tmp.sub[i].vec;
+            const auto& pv = t[j].sub[i].vec;
+            double c = uv[j] / uu[j];
+            for (size_t e = 0; e < tv.size(); ++e) tv[e] = tv[e] + c * pv[e];
+          }
+        for (int i = 0; i < w.num; ++i)
+          for (size_t e = 0; e < w.sub[i].vec.size(); ++e) w.sub[i].vec[e] = w.sub[i].vec[e] - tmp.sub[i].vec[e];
+        wave_normalize(w);
+      }
+      last++;
+      allocate_wave(super, t[last + 1]);
+      model_wave(sys, env, sys_bs, env_bs, t[last], t[last + 1]);
+      alpha1[last] = wave_product(t[last], t[last + 1]);
+      std::vector<double> d(alpha1.begin() + 1, alpha1.begin() + 1 + last);
+      std::vector<double> e(beta1.begin() + 1, beta1.begin() + 1 + last);
+      dstev('N', last, d, e, nullptr);
+      if (std::fabs(d[0] - ritzmin) <= lanzero || (last == loop_in && iter_out == loop_out)) {
+        ritzmin = d[0];
+        lastmin = ritzmin;
+        converged = true;
+        break;
+      }
+      ritzmin = d[0];
+      lastmin = ritzmin;
+    }
+    if (converged) {
+      done = true;
+      break;
+    }
+    // restart: eigen.f90:114-134
+    std::vector<double> d(alpha1.begin() + 1, alpha1.begin() + 1 + last);
+    std::vector<double> e(beta1.begin() + 1, beta1.begin() + 1 + last);
+    std::vector<double> z;
+    dstev('V', last, d, e, &z);
+    ritzmin = d[0];
+    lastmin = ritzmin;
+    for (auto& s : eigvec.sub) std::fill(s.vec.begin(), s.vec.end(), czero);
+    for (int i = 1; i <= last; ++i)
+      for (int x = 0; x < eigvec.num; ++x) {
+        auto& ev = eigvec.sub[x].vec;
+        const auto& tv = t[i].sub[x].vec;
+        for (size_t q = 0; q < ev.size(); ++q) ev[q] = ev[q] + z[(size_t)0 * last + (i - 1)] * tv[q];
+      }
+    wave_normalize(eigvec);
+  }
+  // label 411: eigen.f90:137-160
+  std::vector<double> d(alpha1.begin() + 1, alpha1.begin() + 1 + last);
+  std::vector<double> e(beta1.begin() + 1, beta1.begin() + 1 + last);
+  std::vector<double> z;
+  dstev('V', last, d, e, &z);
+  ritzmin = d[0];
+  for (auto& s : eigvec.sub) std::fill(s.vec.begin(), s.vec.end(), czero);
+  for (int i = 1; i <= last; ++i)
+    for (int x = 0; x < eigvec.num; ++x) {
+      auto& ev = eigvec.sub[x].vec;
+      const auto& tv = t[i].sub[x].vec;
+      double zi = z[(size_t)(i - 1)];
+      for (size_t q = 0; q < ev.size(); ++q) ev[q] = ev[q] + zi * tv[q];
+    }
+  wave_normalize(eigvec);
+  *iters = (iter_out - 1) * loop_in + last;
+  *e0 = ritzmin;
+}
+
+// ---- density matrix (den_mat.f90:4-183), levels=1 ---------------------------------
+void Oracle::density_matrix_sys(const Wave& wave, Block& den) {
+  Wave w = wave;
+  wave_normalize(w);   // Get_density_matrix_sys_new, den_mat.f90:118-124
+  den = Block();
+  den.len = w.sys_len;
+  den.num = w.num;
+  den.sub.assign(den.num, SubBlock());
+  for (int i = 0; i < w.num; ++i) {
+    SubBlock& s = den.sub[i];
+    s.num_up = w.sub[i].sys_num_up;
+    s.num_down = w.sub[i].sys_num_down;
+    s.down_dif = 0;
+    s.row_dim = s.sdim = w.sub[i].sys_dim;
+    den.dim += s.sdim;
+    int sd = w.sub[i].sys_dim, ed = w.sub[i].env_dim;
+    s.mat.assign((size_t)sd * sd, 0.0);
+    zgemm('N', 'C', sd, sd, ed, cone, w.sub[i].vec.data(), sd, w.sub[i].vec.data(), sd, czero,
+          s.mat.data(), sd);
+  }
+}
+
+void Oracle::density_matrix_env(const Wave& wave, Block& den) {
+  Wave w = wave;
+  wave_normalize(w);   // Get_density_matrix_env_new, den_mat.f90:158-164
+  den = Block();
+  den.len = w.env_len;
+  den.num = w.num;
+  den.sub.assign(den.num, SubBlock());
+  for (int i = 0; i < w.num; ++i) {
+    SubBlock& s = den.sub[i];
+    s.num_up = w.sub[i].env_num_up;
+    s.num_down = w.sub[i].env_num_down;
+    s.down_dif = 0;
+    s.row_dim = s.sdim = w.sub[i].env_dim;
+    den.dim += s.sdim;
+    int sd = w.sub[i].sys_dim, ed = w.sub[i].env_dim;
+    s.mat.assign((size_t)ed * ed, 0.0);
+    zgemm('C', 'N', ed, ed, sd, cone, w.sub[i].vec.data(), sd, w.sub[i].vec.data(), sd, czero,
+          s.mat.data(), ed);
+  }
+}
+
+// ---- truncation (den_mat.f90:184-418) ---------------------------------------------
+void Oracle::truncation_operator(const Block& den, Block& trun, double trun_err, int* num_state_out,
+                                 double* err_out, double* ent_out, double* ent_mult_out,
+                                 bool system_block, std::vector<double>* spectrum) {
+  (void)system_block;
+  const double thr = 1.0000000036274937e-15;   // 1.0E-15 (default real), den_mat.f90:278,330
+  int num = den.num;
+  std::vector<std::vector<cplx>> evec(num);
+  std::vector<std::vector<double>> eval(num);
+  std::vector<std::vector<int>> sidx(num);
+  int dim = 0;
+  for (int k = 0; k < num; ++k) {
+    int n = den.sub[k].sdim;
+    evec[k] = den.sub[k].mat;
+    eval[k].assign(n, 0.0);
+    sidx[k].assign(n, 0);
+    if (n > 0) {
+      int lda = n, lwork = 3 * n, info = 0;
+      std::vector<cplx> work(lwork);
+      std::vector<double> rwork(lwork);
+      char jobz = 'V', uplo = 'U';
+      scipy_zheev_(&jobz, &uplo, &n, evec[k].data(), &lda, eval[k].data(), work.data(), &lwork,
+                   rwork.data(), &info);
+    }
+    for (int i = 0; i < n; ++i) sidx[k][i] = dim + i + 1;
+    dim += n;
+  }
+  std::vector<int> idx(dim + 1), eigs(dim + 1);
+  std::vector<double> ev(dim + 1);
+  int p = 0;
+  for (int k = 0; k < num; ++k)
+    for (int i = 0; i < den.sub[k].sdim; ++i) {
+      ++p;
+      idx[p] = sidx[k][i];
+      ev[p] = eval[k][i];
+      eigs[p] = den.sub[k].num_down + 1;
+    }
+  double entropy1 = 0.0;
+  for (int i = 1; i <= dim; ++i)
+    if (ev[i] >= thr) {
+      double v1 = ev[i] / eigs[i];
+      entropy1 = entropy1 - v1 * std::log(v1) * eigs[i];
+    }
+  if (dim >= 1) quicksort_double(ev, idx, 1, dim);
+  double tot = 0.0;
+  for (int i = 1; i <= dim; ++i) tot += ev[i];
+  for (int i = 1; i <= dim; ++i) ev[i] = ev[i] / tot;
+  double tmp_err = 0.0;
+  int num_state;
+  if (dim <= kept_min) {
+    num_state = dim;
+    tmp_err = 0.0;
+  } else {
+    for (int i = kept_min + 1; i <= dim; ++i) tmp_err += ev[i];
+    num_state = kept_min;
+    while (tmp_err > trun_err) {
+      num_state++;
+      tmp_err = tmp_err - ev[num_state];
+      if (tmp_err <= trun_err || num_state >= kept_max) break;
+    }
+  }
+  double entropys = 0.0;
+  for (int i = 1; i <= dim; ++i)
+    if (ev[i] >= thr) entropys = entropys - ev[i] * std::log(ev[i]);
+  std::vector<int> tmpidx(num, 0);
+  for (int k = 1; k <= num_state; ++k) {
+    bool f = false;
+    for (int i = 0; i < num && !f; ++i)
+      for (int x = 0; x < den.sub[i].sdim; ++x)
+        if (sidx[i][x] == idx[k]) {
+          tmpidx[i]++;
+          f = true;
+          break;
+        }
+  }
+  trun = Block();
+  for (int i = 0; i < num; ++i) {
+    if (tmpidx[i] <= 0) continue;
+    SubBlock s;
+    s.num_up = den.sub[i].num_up;
+    s.num_down = den.sub[i].num_down;
+    s.down_dif = 0;
+    s.row_dim = den.sub[i].sdim;
+    s.sdim = tmpidx[i];
+    s.mat.assign((size_t)s.row_dim * s.sdim, 0.0);
+    int row = s.row_dim, col = s.sdim;
+    for (int c = 0; c < col; ++c)
+      for (int r = 0; r < row; ++r) s.at(r, c) = evec[i][(size_t)(row - col + c) * row + r];
+    trun.sub.push_back(std::move(s));
+  }
+  trun.num = (int)trun.sub.size();
+  trun.len = den.len;
+  trun.up_dif = den.up_dif;
+  trun.down_dif = den.down_dif;
+  trun.dim = 0;
+  for (auto& s : trun.sub) trun.dim += s.sdim;
+  *num_state_out = num_state;
+  *err_out = tmp_err;
+  *ent_out = entropys;
+  *ent_mult_out = entropy1;
+  if (spectrum) spectrum->assign(ev.begin() + 1, ev.end());
+}
+
+// ---- wave transformations (dmrg_sub.f90:1471-1789) --------------------------------
+void Oracle::wave_trans_LR(const Basis& sys_bs, const Basis& env_bs, const Block& sys_trun,
+                           const Block& env_trun, const Wave& old_w, Wave& new_w) {
+  std::vector<cplx> sub;
+  for (int i = 0; i < old_w.num; ++i) {
+    const SubWave& o = old_w.sub[i];
+    int st_id = find_blk(sys_trun, o.sys_num_up, o.sys_num_down);
+    if (st_id < 0) continue;
+    for (int k = 0; k < env_bs.num; ++k) {
+      if (env_bs.sub[k].new_num_up != o.env_num_up || env_bs.sub[k].new_num_down != o.env_num_down) continue;
+      for (const auto& p : env_bs.sub[k].sub) {
+        int et_id = find_blk(env_trun, p.bl_num_up, p.bl_num_down);
+        int neu = p.bl_num_up, ned = p.bl_num_down;
+        for (int nsd = std::abs(o.sys_num_down - p.st_num_down); nsd <= o.sys_num_down + p.st_num_down;
+             nsd += 2) {
+          int nsu = o.sys_num_up + p.st_num_up;
+          int y = find_bs(sys_bs, nsu, nsd);
+          const SubBasisMap* q = nullptr;
+          if (y >= 0)
+            for (const auto& qq : sys_bs.sub[y].sub)
+              if (qq.bl_num_up == o.sys_num_up && qq.bl_num_down == o.sys_num_down &&
+                  qq.st_num_up == p.st_num_up && qq.st_num_down == p.st_num_down) {
+                q = &qq;
+                break;
+              }
+          int nw = -1;
+          for (int yy = 0; yy < new_w.num; ++yy) {
+            const SubWave& s = new_w.sub[yy];
+            if (s.sys_num_up == nsu && s.sys_num_down == nsd && s.env_num_up == neu && s.env_num_down == ned) {
+              nw = yy;
+              break;
+            }
+          }
+          if (et_id < 0 || !q || nw < 0) continue;
+          SubWave& n = new_w.sub[nw];
+          int new_env_dim = n.env_dim, new_pos = q->spos, nsub = q->sdim;
+          int j12 = o.sys_num_down, j3 = p.st_num_down, j4 = ned, j123 = nsd, j34 = o.env_num_down;
+          double c11 = pm1((j12 + j3 + j123) / 2) / std::sqrt((1.0 + j12) * (1.0 + j123));
+          if (c11 == 0.0) continue;
+          c11 = c11 * std::sqrt((1.0 + j123) * (j34 + 1.0));
+          if (((j12 + j3 + j4) / 2) % 2 != 0) c11 = -c11;
+          if (((j3 + j4 - j34) / 2) % 2 != 0) c11 = -c11;
+          cplx coef1 = c11;
+          int osd = o.sys_dim, opos = p.spos, osub = p.sdim;
+          sub.assign((size_t)nsub * osub, 0.0);
+          zgemm('C', 'N', nsub, osub, osd, coef1, sys_trun.sub[st_id].mat.data(), osd,
+                &o.vec[(size_t)opos * osd], osd, czero, sub.data(), nsub);
+          zgemm('N', 'C', nsub, new_env_dim, osub, cone, sub.data(), nsub,
+                env_trun.sub[et_id].mat.data(), new_env_dim, cone, &n.vec[new_pos], n.sys_dim);
+        }
+      }
+    }
+  }
+  wave_normalize(new_w);
+}
+
+void Oracle::wave_trans_RL(const Basis& sys_bs, const Basis& env_bs, const Block& sys_trun,
+                           const Block& env_trun, const Wave& old_w, Wave& new_w) {
+  std::vector<cplx> sub;
+  for (int i = 0; i < old_w.num; ++i) {
+    const SubWave& o = old_w.sub[i];
+    int et_id = find_blk(env_trun, o.env_num_up, o.env_num_down);
+    if (et_id < 0) continue;
+    for (int k = 0; k < sys_bs.num; ++k) {
+      if (sys_bs.sub[k].new_num_up != o.sys_num_up || sys_bs.sub[k].new_num_down != o.sys_num_down) continue;
+      for (const auto& p : sys_bs.sub[k].sub) {
+        int nsu = p.bl_num_up, nsd = p.bl_num_down;
+        for (int ned = std::abs(o.env_num_down - p.st_num_down); ned <= o.env_num_down + p.st_num_down;
+             ned += 2) {
+          int neu = o.env_num_up + p.st_num_up;
+          int st_id = find_blk(sys_trun, nsu, nsd);
+          int y = find_bs(env_bs, neu, ned);
+          const SubBasisMap* q = nullptr;
+          if (y >= 0)
+            for (const auto& qq : env_bs.sub[y].sub)
+              if (qq.bl_num_up == o.env_num_up && qq.bl_num_down == o.env_num_down &&
+                  qq.st_num_up == p.st_num_up && qq.st_num_down == p.st_num_down) {
+                q = &qq;
+                break;
+              }
+          int nw = -1;
+          for (int yy = 0; yy < new_w.num; ++yy) {
+            const SubWave& s = new_w.sub[yy];
+            if (s.sys_num_up == nsu && s.sys_num_down == nsd && s.env_num_up == neu && s.env_num_down == ned) {
+              nw = yy;
+              break;
+            }
+          }
+          if (st_id < 0 || !q || nw < 0) continue;
+          SubWave& n = new_w.sub[nw];
+          int new_sys_dim = n.sys_dim, new_pos = q->spos, nsub = q->sdim;
+          int j12 = o.env_num_down, j3 = p.st_num_down, j4 = nsd, j123 = ned, j34 = o.sys_num_down;
+          double c11 = pm1((j34 + j4 + j3) / 2) / std::sqrt((1.0 + j12) * (1.0 + j4));
+          if (c11 == 0.0) continue;
+          c11 = c11 * std::sqrt((1.0 + j123) * (j34 + 1.0));
+          if (((j4 + j3 + j12) / 2) % 2 != 0) c11 = -c11;
+          if (((j12 + j3 - j123) / 2) % 2 != 0) c11 = -c11;
+          cplx coef1 = c11;
+          int oed = o.env_dim, opos = p.spos, osub = p.sdim;
+          sub.assign((size_t)new_sys_dim * oed, 0.0);
+          zgemm('N', 'N', new_sys_dim, oed, osub, coef1, sys_trun.sub[st_id].mat.data(), new_sys_dim,
+                &o.vec[opos], o.sys_dim, czero, sub.data(), new_sys_dim);
+          zgemm('N', 'N', new_sys_dim, nsub, oed, cone, sub.data(), new_sys_dim,
+                env_trun.sub[et_id].mat.data(), oed, cone, &n.vec[(size_t)new_pos * n.sys_dim], n.sys_dim);
+        }
+      }
+    }
+  }
+  wave_normalize(new_w);
+}
+
+// ---- block growth (get_sys.f90:4-592) ---------------------------------------------
+void Oracle::hamiltonian_sys(Model& pre, const Basis& basis, const Block& trun) {
+  Model next;
+  next.len = pre.len + 1;
+  next.sub.assign(L.num_site + 1, BlockSet());
+  update_block_dia(pre.ham, basis, next.ham);
+  Block tmp, tmp1, tt;
+  const int ijs[3] = {1, 3, 5};
+  for (int ij : ijs) {
+    int j = pre.len + 1;
+    for (int k = 1; k <= L.neibt; ++k) {
+      int I = L.NEIB(j, k);
+      if (I <= pre.len && I > 0) {
+        int i1 = L.INB1(I, pre.len);
+        if (i1 > 0 && i1 <= L.nleg11[pre.len]) {
+          cplx cx = L.JT(k, j), csd = L.JD(k, j);
+          if (ij == 1 && cx != 0.0) {
+            block_transfer_trans(st_elec_down, tt);
+            hamiltonian_ndia(pre.sub[i1].elec_up, tt, basis, cx, next.ham, 'F', 'S');
+          }
+          if (ij == 3 && csd != 0.0) hamiltonian_ndia(pre.sub[i1].spin_sd, st_sd, basis, csd, next.ham, 'B', 'S');
+        }
+      }
+    }
+    for (int y = 1; y <= pre.len; ++y) {
+      int i1 = L.INB1(y, pre.len);
+      if (i1 <= L.nleg11[pre.len]) {
+        if (ij == 1) {
+          update_block_ndia(pre.sub[i1].elec_up, basis, next.sub[i1].elec_up, 'F', false);
+          update_block_ndia(pre.sub[i1].elec_down, basis, next.sub[i1].elec_down, 'F', false);
+          pre.sub[i1].elec_up = Block();
+          pre.sub[i1].elec_down = Block();
+        }
+        if (ij == 3) {
+          update_block_ndia(pre.sub[i1].spin_sd, basis, next.sub[i1].spin_sd, 'B', false);
+          pre.sub[i1].spin_sd = Block();
+        }
+        if (ij == 5) {
+          update_block_dia(pre.sub[i1].num_sn, basis, next.sub[i1].num_sn);
+          pre.sub[i1].num_sn = Block();
+        }
+      }
+    }
+    if (ij == 1) {
+      update_site_ndia(st_elec_up, basis, tmp, 'F', false);
+      update_site_ndia(st_elec_down, basis, tmp1, 'F', false);
+    }
+    if (ij == 3) update_site_ndia(st_sd, basis, tmp, 'B', false);
+    if (ij == 5) update_site_dia(num_elec, basis, tmp);
+    for (int k = 1; k <= L.neibt; ++k) {
+      int I = L.NEIB(j, k);
+      if (I <= pre.len && I > 0) {
+        int i1 = L.INB1(I, pre.len);
+        if (i1 > 0 && i1 <= L.nleg11[pre.len]) {
+          cplx csn = L.JN(k, j);
+          if (ij == 5 && csn != 0.0) hamiltonian_dia(next.sub[i1].num_sn, tmp, csn, next.ham);
+        }
+      }
+    }
+    int nleg1 = L.nleg11[pre.len + 1];
+    for (int I = 1; I <= pre.len; ++I) {
+      int i1 = L.INB1(I, pre.len), J = L.INB1(I, pre.len + 1);
+      if (J <= nleg1 && J != i1) {
+        if (ij == 1) {
+          next.sub[J].elec_up = next.sub[i1].elec_up;
+          next.sub[J].elec_down = next.sub[i1].elec_down;
+        }
+        if (ij == 3) next.sub[J].spin_sd = next.sub[i1].spin_sd;
+        if (ij == 5) next.sub[J].num_sn = next.sub[i1].num_sn;
+      }
+    }
+    int jn = L.INB1(pre.len + 1, pre.len + 1);
+    if (ij == 1) {
+      next.sub[jn].elec_up = tmp;
+      next.sub[jn].elec_down = tmp1;
+    }
+    if (ij == 3) next.sub[jn].spin_sd = tmp;
+    if (ij == 5) next.sub[jn].num_sn = tmp;
+    for (int jj = nleg1 + 1; jj <= L.nleg11[pre.len]; ++jj) {
+      if (ij == 1) next.sub[jj].elec_up = next.sub[jj].elec_down = Block();
+      if (ij == 3) next.sub[jj].spin_sd = Block();
+      if (ij == 5) next.sub[jj].num_sn = Block();
+    }
+    for (int ii = 1; ii <= L.nleg11[next.len]; ++ii) {
+      if (ij == 1) {
+        update_trun_ndia(next.sub[ii].elec_up, pre.sub[ii].elec_up, trun);
+        update_trun_ndia(next.sub[ii].elec_down, pre.sub[ii].elec_down, trun);
+        next.sub[ii].elec_up = next.sub[ii].elec_down = Block();
+      }
+      if (ij == 3) {
+        update_trun_ndia(next.sub[ii].spin_sd, pre.sub[ii].spin_sd, trun);
+        next.sub[ii].spin_sd = Block();
+      }
+      if (ij == 5) {
+        update_trun_dia(next.sub[ii].num_sn, pre.sub[ii].num_sn, trun);
+        next.sub[ii].num_sn = Block();
+      }
+    }
+  }
+  Block h;
+  update_trun_dia(next.ham, h, trun);
+  pre.ham = h;
+  pre.len = next.len;
+}
+
+void Oracle::hamiltonian_env(Model& pre, const Basis& basis, const Block& trun) {
+  Model next;
+  next.len = pre.len + 1;
+  next.sub.assign(L.num_site + 1, BlockSet());
+  update_block_dia(pre.ham, basis, next.ham);
+  Block tmp, tmp1, tt;
+  const int ijs[3] = {1, 3, 5};
+  int j = pre.len + 1 + mshift;
+  int lat = L.nposi_lat[j];
+  for (int ij : ijs) {
+    for (int k = 1; k <= L.neibt; ++k) {
+      int I = L.NEIB(lat, k);
+      int II = L.nposi_dm[I] - mshift;
+      if (II <= pre.len && II > 0) {
+        int i1 = L.INB1(II, pre.len);
+        if (i1 > 0 && i1 <= L.nleg11[pre.len]) {
+          cplx cx = L.JT(k, lat), csd = L.JD(k, lat);
+          if (ij == 1 && cx != 0.0) {
+            block_transfer_trans(st_elec_up, tt);
+            hamiltonian_ndia(pre.sub[i1].elec_down, tt, basis, cx, next.ham, 'F', 'E');
+          }
+          if (ij == 3 && csd != 0.0) hamiltonian_ndia(pre.sub[i1].spin_sd, st_sd, basis, csd, next.ham, 'B', 'E');
+        }
+      }
+    }
+    for (int y = 1; y <= pre.len; ++y) {
+      int i1 = L.INB1(y, pre.len);
+      if (i1 <= L.nleg11[pre.len]) {
+        if (ij == 1) {
+          update_block_ndia(pre.sub[i1].elec_up, basis, next.sub[i1].elec_up, 'F', true);
+          update_block_ndia(pre.sub[i1].elec_down, basis, next.sub[i1].elec_down, 'F', true);
+          pre.sub[i1].elec_up = Block();
+          pre.sub[i1].elec_down = Block();
+        }
+        if (ij == 3) {
+          update_block_ndia(pre.sub[i1].spin_sd, basis, next.sub[i1].spin_sd, 'B', true);
+          pre.sub[i1].spin_sd = Block();
+        }
+        if (ij == 5) {
+          update_block_dia(pre.sub[i1].num_sn, basis, next.sub[i1].num_sn);
+          pre.sub[i1].num_sn = Block();
+        }
+      }
+    }
+    if (ij == 1) {
+      update_site_ndia(st_elec_up, basis, tmp, 'F', true);
+      update_site_ndia(st_elec_down, basis, tmp1, 'F', true);
+    }
+    if (ij == 3) update_site_ndia(st_sd, basis, tmp, 'B', true);
+    if (ij == 5) update_site_dia(num_elec, basis, tmp);
+    for (int k = 1; k <= L.neibt; ++k) {
+      int I = L.NEIB(lat, k);
+      int II = L.nposi_dm[I] - mshift;
+      if (II <= pre.len && II > 0) {
+        int i1 = L.INB1(II, pre.len);
+        if (i1 > 0 && i1 <= L.nleg11[pre.len]) {
+          cplx csn = L.JN(k, lat);
+          if (ij == 5 && csn != 0.0) hamiltonian_dia(next.sub[i1].num_sn, tmp, csn, next.ham);
+        }
+      }
+    }
+    int nleg1 = L.nleg11[pre.len + 1];
+    for (int I = 1; I <= pre.len; ++I) {
+      int i1 = L.INB1(I, pre.len), J = L.INB1(I, pre.len + 1);
+      if (J <= nleg1 && J != i1) {
+        if (ij == 1) {
+          next.sub[J].elec_up = next.sub[i1].elec_up;
+          next.sub[J].elec_down = next.sub[i1].elec_down;
+        }
+        if (ij == 3) next.sub[J].spin_sd = next.sub[i1].spin_sd;
+        if (ij == 5) next.sub[J].num_sn = next.sub[i1].num_sn;
+      }
+    }
+    int jn = L.INB1(pre.len + 1, pre.len + 1);
+    if (ij == 1) {
+      next.sub[jn].elec_up = tmp;
+      next.sub[jn].elec_down = tmp1;
+    }
+    if (ij == 3) next.sub[jn].spin_sd = tmp;
+    if (ij == 5) next.sub[jn].num_sn = tmp;
+    for (int jj = nleg1 + 1; jj <= L.nleg11[pre.len]; ++jj) {
+      if (ij == 1) next.sub[jj].elec_up = next.sub[jj].elec_down = Block();
+      if (ij == 3) next.sub[jj].spin_sd = Block();
+      if (ij == 5) next.sub[jj].num_sn = Block();
+    }
+    for (int ii = 1; ii <= L.nleg11[next.len]; ++ii) {
+      if (ij == 1) {
+        update_trun_ndia(next.sub[ii].elec_up, pre.sub[ii].elec_up, trun);
+        update_trun_ndia(next.sub[ii].elec_down, pre.sub[ii].elec_down, trun);
+        next.sub[ii].elec_up = next.sub[ii].elec_down = Block();
+      }
+      if (ij == 3) {
+        update_trun_ndia(next.sub[ii].spin_sd, pre.sub[ii].spin_sd, trun);
+        next.sub[ii].spin_sd = Block();
+      }
+      if (ij == 5) {
+        update_trun_dia(next.sub[ii].num_sn, pre.sub[ii].num_sn, trun);
+        next.sub[ii].num_sn = Block();
+      }
+    }
+  }
+  Block h;
+  update_trun_dia(next.ham, h, trun);
+  pre.ham = h;
+  pre.len = next.len;
+}
+
+}  // namespace orc

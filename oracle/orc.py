@@ -1,0 +1,137 @@
+"""ctypes wrapper of the oracle (oracle/_build/liborc.so).
+
+TEST INFRASTRUCTURE ONLY: the oracle is the CPU restatement of the reference
+DMRG hot path (hyx15903/TSC_Tri_t1t2J1J2, DMRG_code/*.f90).  Only tests/,
+``__graft_entry__.smoke`` and bench.py's cpu_baseline leg may import it, and
+only as the checker / CPU baseline, never as the thing measured or shipped.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+from dataclasses import dataclass, field
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_build", "liborc.so")
+
+_lib = None
+
+
+def build(force: bool = False) -> str:
+    """Compile the oracle with its Makefile (g++ + scipy's OpenBLAS)."""
+    if force or not os.path.exists(LIB_PATH):
+        subprocess.run(["make", "-s", "-C", HERE], check=True)
+    return LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        build()
+        L = ctypes.CDLL(LIB_PATH)
+        vp, i, d = ctypes.c_void_p, ctypes.c_int, ctypes.c_double
+        L.orc_new.restype = vp
+        L.orc_new.argtypes = [i, i, d, d, d, d, i, i, i, ctypes.POINTER(i), i, d, ctypes.c_ulonglong, i]
+        L.orc_free.argtypes = [vp]
+        L.orc_error.restype = ctypes.c_char_p
+        L.orc_error.argtypes = [vp]
+        L.orc_run.argtypes = [vp]
+        L.orc_run.restype = i
+        L.orc_tot_num_up.argtypes = [vp]
+        L.orc_steps.argtypes = [vp, ctypes.POINTER(d)]
+        L.orc_capture_serialize.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong)]
+        L.orc_serialized_copy.argtypes = [vp, ctypes.POINTER(i), ctypes.POINTER(d)]
+        L.orc_w6js.restype = d
+        L.orc_w6js.argtypes = [i] * 6
+        L.orc_w3js.restype = d
+        L.orc_w3js.argtypes = [i] * 6
+        L.orc_hpsi_flat.argtypes = [vp, i, i, ctypes.POINTER(i), ctypes.POINTER(d), ctypes.POINTER(d), i,
+                                    ctypes.POINTER(d), ctypes.POINTER(d)]
+        L.orc_hpsi_flat.restype = i
+        _lib = L
+    return _lib
+
+
+@dataclass
+class RunConfig:
+    """Model and schedule (restates main.f90:54-99 as data)."""
+    Nx: int = 6
+    Ny: int = 4
+    t1: float = 1.0
+    t2: float = 0.0
+    J1: float = 0.4
+    J2: float = 0.0
+    delta: int = 12
+    kept_min: int = 100
+    kept_warm: int = 100
+    sweeps: list = field(default_factory=lambda: [100])
+    lanzero: float = -1.0      # >0 overrides the reference's Lanczos tolerance schedule
+    seed: int = 1
+
+
+STEP_FIELDS = ["phase", "sys_len", "env_len", "e0", "iters", "num_state", "trun_err",
+               "entropy", "entropy_mult", "hpsi_calls", "hpsi_seconds", "hpsi_flops"]
+
+
+class Oracle:
+    def __init__(self, cfg: RunConfig, capture_step: int = -1):
+        L = lib()
+        sk = (ctypes.c_int * max(1, len(cfg.sweeps)))(*cfg.sweeps)
+        self.h = L.orc_new(cfg.Nx, cfg.Ny, cfg.t1, cfg.t2, cfg.J1, cfg.J2, cfg.delta, cfg.kept_min,
+                           cfg.kept_warm, sk, len(cfg.sweeps), cfg.lanzero, cfg.seed, capture_step)
+        err = L.orc_error(self.h)
+        if err:
+            raise RuntimeError(err.decode())
+        self.cfg = cfg
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().orc_free(self.h)
+            self.h = None
+
+    def run(self) -> list[dict]:
+        L = lib()
+        n = L.orc_run(self.h)
+        if n < 0:
+            raise RuntimeError(L.orc_error(self.h).decode())
+        buf = np.zeros(12 * max(n, 1), dtype=np.float64)
+        L.orc_steps(self.h, buf.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+        return [dict(zip(STEP_FIELDS, buf[12 * k:12 * k + 12].tolist())) for k in range(n)]
+
+    def capture(self):
+        """Flat (ints, complex) serialisation of the captured superblock."""
+        L = lib()
+        ni, nc = ctypes.c_longlong(), ctypes.c_longlong()
+        if L.orc_capture_serialize(self.h, ctypes.byref(ni), ctypes.byref(nc)) != 0:
+            raise RuntimeError("no capture")
+        ints = np.zeros(ni.value, dtype=np.int32)
+        data = np.zeros(nc.value, dtype=np.complex128)
+        L.orc_serialized_copy(self.h, ints.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                              data.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+        return ints, data
+
+    def hpsi_flat(self, sys_len, env_len, ints, data, npsi, nreps=1):
+        """model_wave on a flat superblock (sys model, env model, bases, psi)."""
+        L = lib()
+        ints = np.ascontiguousarray(ints, dtype=np.int32)
+        data = np.ascontiguousarray(data, dtype=np.complex128)
+        out = np.zeros(npsi, dtype=np.complex128)
+        sec, flops = ctypes.c_double(), ctypes.c_double()
+        rc = L.orc_hpsi_flat(self.h, sys_len, env_len, ints.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                             data.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                             out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), nreps,
+                             ctypes.byref(sec), ctypes.byref(flops))
+        if rc != 0:
+            raise RuntimeError(L.orc_error(self.h).decode())
+        return out, sec.value, flops.value
+
+
+def w6js(*a) -> float:
+    return lib().orc_w6js(*[int(x) for x in a])
+
+
+def w3js(*a) -> float:
+    return lib().orc_w3js(*[int(x) for x in a])

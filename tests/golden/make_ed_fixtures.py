@@ -1,0 +1,171 @@
+"""Exact-diagonalisation known answers for the t1-t2-J1-J2 model on small
+triangular cylinders, plus sympy Wigner-6j values.
+
+These pin the oracle's physics where the reference itself cannot run (no Fortran
+compiler): a DMRG that keeps every multiplet must reproduce the lowest S=0
+energy of the full many-body Hamiltonian
+
+    H = sum_<ij> [ -t_ij sum_s (c+_is c_js + h.c.) + J_ij (S_i.S_j - n_i n_j / 4) ]
+
+on the same lattice.  Lattice (restating dmrg_sub.f90:453-583): sites
+i = (x-1)*Ny + y, periodic in y, open in x; nearest neighbours along (0,1),
+(1,0), (1,-1) carry (t1, J1); next-nearest along (1,1), (2,-1), (1,-2) carry
+(t2, J2).  Electron count from main.f90:93-99.  Run:  python make_ed_fixtures.py
+"""
+from __future__ import annotations
+
+import itertools
+import json
+import os
+
+import numpy as np
+import scipy.sparse as sp
+import scipy.sparse.linalg as sla
+
+
+def bonds(Nx, Ny):
+    def idx(x, y):
+        return (x - 1) * Ny + ((y - 1) % Ny) + 1
+    nn, nnn = set(), set()
+    for x in range(1, Nx + 1):
+        for y in range(1, Ny + 1):
+            i = idx(x, y)
+            for dx, dy, kind in [(0, 1, 1), (1, 0, 1), (1, -1, 1), (1, 1, 2), (2, -1, 2), (1, -2, 2)]:
+                if x + dx > Nx:
+                    continue
+                j = idx(x + dx, y + dy)
+                if j == i:
+                    continue
+                b = (min(i, j), max(i, j))
+                (nn if kind == 1 else nnn).add(b)
+    nnn -= nn
+    return sorted(nn), sorted(nnn)
+
+
+def n_electrons(ns, delta=12):
+    return 2 * (ns // 2 - (ns + 2 * delta - 1) // (2 * delta))
+
+
+def tj_ground_state(Nx, Ny, t1, t2, J1, J2, sign_t=-1.0, penalty=10.0):
+    ns = Nx * Ny
+    ne = n_electrons(ns)
+    nup = ne // 2
+    # basis: (up mask, down mask), no double occupancy, Sz = 0
+    states = []
+    for occ in itertools.combinations(range(ns), ne):
+        for ups in itertools.combinations(occ, nup):
+            um = sum(1 << q for q in ups)
+            dm = sum(1 << q for q in occ) ^ um
+            states.append((um, dm))
+    index = {s: k for k, s in enumerate(states)}
+    nn, nnn = bonds(Nx, Ny)
+    blist = [(i - 1, j - 1, t1, J1) for i, j in nn] + [(i - 1, j - 1, t2, J2) for i, j in nnn]
+
+    # fermion ordering: modes (site, spin) -> 2*site + spin
+    def occ_modes(um, dm):
+        m = 0
+        for q in range(ns):
+            if (um >> q) & 1:
+                m |= 1 << (2 * q)
+            if (dm >> q) & 1:
+                m |= 1 << (2 * q + 1)
+        return m
+
+    def hop_sign(mode_mask, a, b):
+        lo, hi = min(a, b), max(a, b)
+        between = mode_mask & (((1 << hi) - 1) ^ ((1 << (lo + 1)) - 1))
+        return -1.0 if bin(between).count("1") % 2 else 1.0
+
+    rows, cols, vals = [], [], []
+    srows, scols, svals = [], [], []
+    for k, (um, dm) in enumerate(states):
+        mm = occ_modes(um, dm)
+        diag = 0.0
+        for i, j, t, J in blist:
+            ni = ((um >> i) | (dm >> i)) & 1
+            nj = ((um >> j) | (dm >> j)) & 1
+            szi = 0.5 * (((um >> i) & 1) - ((dm >> i) & 1))
+            szj = 0.5 * (((um >> j) & 1) - ((dm >> j) & 1))
+            diag += J * (szi * szj - 0.25 * ni * nj)
+            # spin flip S+_i S-_j + S-_i S+_j (no fermion sign for a swap of adjacent spins of one pair)
+            if ni and nj and (((um >> i) & 1) != ((um >> j) & 1)) and J != 0.0:
+                num, ndm = um ^ (1 << i) ^ (1 << j), dm ^ (1 << i) ^ (1 << j)
+                # express as c+_{i s'} c_{i s} c+_{j s} c_{j s'} with explicit Jordan-Wigner signs
+                s_i = 0 if (um >> i) & 1 else 1
+                s_j = 1 - s_i
+                m1 = mm
+                sg = 1.0
+                for (ann, cre) in [(2 * j + s_j, 2 * j + s_i), (2 * i + s_i, 2 * i + s_j)]:
+                    sg *= hop_sign(m1, ann, cre)
+                    m1 = (m1 ^ (1 << ann)) | (1 << cre)
+                rows.append(index[(num, ndm)]); cols.append(k); vals.append(0.5 * J * sg)
+            # hopping
+            if t != 0.0:
+                for s, msk in ((0, um), (1, dm)):
+                    for a, b in ((i, j), (j, i)):
+                        if ((msk >> b) & 1) and not (((um >> a) | (dm >> a)) & 1):
+                            ma, mb = 2 * a + s, 2 * b + s
+                            sg = hop_sign(mm, mb, ma)
+                            if s == 0:
+                                nstate = (um ^ (1 << a) ^ (1 << b), dm)
+                            else:
+                                nstate = (um, dm ^ (1 << a) ^ (1 << b))
+                            rows.append(index[nstate]); cols.append(k); vals.append(sign_t * t * sg)
+        rows.append(k); cols.append(k); vals.append(diag)
+        # total S^2 = (Sz)^2 + (S+S- + S-S+)/2 ; Sz = 0 here -> S^2 = sum_ij (Sz_i Sz_j + (S+_i S-_j + h.c.)/2)
+        sz = [0.5 * (((um >> q) & 1) - ((dm >> q) & 1)) for q in range(ns)]
+        s2d = sum(sz[a] * sz[b] for a in range(ns) for b in range(ns))
+        s2d += sum(0.5 for q in range(ns) if ((um | dm) >> q) & 1)   # S+_i S-_i + S-_i S+_i halves on site
+        srows.append(k); scols.append(k); svals.append(s2d)
+        for a in range(ns):
+            for b in range(ns):
+                if a == b:
+                    continue
+                if ((um >> b) & 1) and ((dm >> a) & 1):   # S+_a S-_b : a down->up, b up->down
+                    num, ndm = um ^ (1 << a) ^ (1 << b), dm ^ (1 << a) ^ (1 << b)
+                    m1, sg = mm, 1.0
+                    for (ann, cre) in [(2 * b, 2 * b + 1), (2 * a + 1, 2 * a)]:
+                        sg *= hop_sign(m1, ann, cre)
+                        m1 = (m1 ^ (1 << ann)) | (1 << cre)
+                    srows.append(index[(num, ndm)]); scols.append(k); svals.append(sg)
+    n = len(states)
+    H = sp.csr_matrix((vals, (rows, cols)), shape=(n, n))
+    S2 = sp.csr_matrix((svals, (srows, scols)), shape=(n, n))
+    Hp = H + penalty * S2
+    w, v = sla.eigsh(Hp, k=1, which="SA", tol=1e-13, maxiter=100000)
+    e = float(w[0])
+    s2 = float(np.real(v[:, 0].conj() @ (S2 @ v[:, 0])))
+    return {"Nx": Nx, "Ny": Ny, "t1": t1, "t2": t2, "J1": J1, "J2": J2, "n_sites": ns,
+            "n_electrons": ne, "dim": n, "e0_S0": e - penalty * s2, "S2": s2, "sign_t": sign_t}
+
+
+def main():
+    out = {"ed": [], "w6j": []}
+    cases = [(2, 4, 1.0, 0.0, 0.4, 0.0), (2, 4, 1.0, 0.3, 0.4, 0.036), (3, 4, 1.0, 0.0, 0.4, 0.0),
+             (3, 4, 1.0, 0.3, 0.4, 0.036)]
+    for c in cases:
+        r = tj_ground_state(*c)
+        print(r)
+        out["ed"].append(r)
+    from sympy.physics.wigner import wigner_6j
+    from sympy import Rational
+    rng = np.random.default_rng(7)
+    count = 0
+    while count < 60:
+        j = [int(x) for x in rng.integers(0, 9, size=6)]
+        try:
+            val = wigner_6j(*[Rational(x, 2) for x in j])
+        except ValueError:   # sympy rejects non-triangular arguments; the symbol is zero
+            val = 0
+        if val == 0 and rng.random() < 0.8:
+            continue
+        out["w6j"].append({"args2": j, "value": float(val)})
+        count += 1
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "ed_and_6j.json")
+    with open(path, "w") as f:
+        json.dump(out, f, indent=1)
+    print("wrote", path)
+
+
+if __name__ == "__main__":
+    main()
