@@ -1,0 +1,151 @@
+/*
+ * tsc_gpu.h -- C-ABI of the B200 superblock engine for the SU(2) two-site DMRG of
+ * the t1-t2-J1-J2 model on triangular cylinders (drop-in for the hot path of
+ * hyx15903/TSC_Tri_t1t2J1J2, DMRG_code/*.f90).
+ *
+ * Layout contract (the reference's derived types flattened, DMRG_code/common.f90:84-156):
+ *   Block  (Total_Block):  ints  [len, num, dim, up_dif, down_dif]
+ *                          then num x [num_up, num_down, down_dif, row_dim, sdim]
+ *                          data  concatenated column-major complex128 sub-block matrices
+ *   Basis  (Total_Basis):  ints  [len, num, dim], num x [new_num_up, new_num_down, dim, npieces],
+ *                          then all pieces x [bl_num_up, bl_num_down, st_num_up, st_num_down, spos, sdim]
+ *   Wave   (Wavefunction): ints  [sys_len, env_len, num, dim]
+ *                          then num x [sys_num_up, sys_num_down, env_num_up, env_num_down, sys_dim, env_dim]
+ *                          data  concatenated column-major complex128 sectors
+ *   Model  (Total_Model):  ints  [len, nops], Block ham, then for op = 1..nops the four
+ *                          Blocks elec_up, elec_down, spin_sd, num_sn of boundary site op
+ * Complex data is interleaved (re, im) double pairs, in the element order of the
+ * Fortran mat/vec arrays.  The caller owns every host buffer; the library owns
+ * device-resident copies per context and never frees caller memory.
+ *
+ * Every entry point returns 0 on success or a negative TSC_E* status; it never
+ * aborts the host process.  tsc_last_error() gives a one-line reason.
+ * One host thread per context; distinct contexts are independent.
+ */
+#ifndef TSC_GPU_H
+#define TSC_GPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TSC_OK 0
+#define TSC_E_ARG -1        /* bad argument / descriptor */
+#define TSC_E_QN -2         /* quantum-number mismatch (reference stops, get_sys.f90:3166-3168) */
+#define TSC_E_CUDA -3       /* CUDA runtime / library failure */
+#define TSC_E_STATE -4      /* call out of order (no superblock set, ...) */
+#define TSC_E_NOMEM -5      /* device allocation failed */
+#define TSC_E_LIMIT -6      /* size above a documented limit */
+
+/* Model: lattice and couplings (main.f90:59-99, dmrg_setup dmrg_sub.f90:334-644). */
+typedef struct tsc_model_config {
+  int Nx, Ny;              /* YC cylinder: Ny legs periodic in y, Nx columns open in x */
+  double t1, t2, J1, J2;   /* jt=-t*sqrt(2), jz=J, jd=-sqrt(3)*J, jn=-J/4 on bonds 1-6 / 7-12 */
+  int delta;               /* inverse hole doping; electrons from main.f90:93-99 */
+  int device;              /* CUDA device ordinal */
+} tsc_model_config;
+
+/* Sweep schedule (main.f90:114-209, dmrg_sub.f90:974-1465). */
+typedef struct tsc_sweep_config {
+  int kept_min;            /* den_mat.f90:299-318 */
+  int kept_max_warmup;     /* kept_max of warm-up and the first two half sweeps */
+  int nsweeps;
+  const int* sweep_kept_max;   /* nsweeps entries */
+  double lanzero;          /* >0: Lanczos tolerance in every phase; <=0: reference schedule */
+  unsigned long long seed; /* random initial states (block.f90:1154-1180 stand-in) */
+} tsc_sweep_config;
+
+/* One record per Lanczos solve (eigen.f90:169-173, den_mat.f90:342-350). */
+typedef struct tsc_step_log {
+  int phase;               /* 0 warm-up, 1 left_to_right, 2 right_to_left */
+  int sys_len, env_len;
+  double e0;
+  int lanczos_iters;
+  int num_state;
+  double trun_err, entropy, entropy_mult;
+  int hpsi_calls;
+  double hpsi_seconds;     /* device time of the H.psi launches of this solve */
+  double hpsi_flops;       /* algorithmic flops (reference association order) */
+  double step_seconds;     /* wall time of the whole DMRG step on the device */
+} tsc_step_log;
+
+typedef struct tsc_ctx tsc_ctx;
+
+/* Replaces the global set-up of main.f90:29-99 (Get_Lattice, site operators,
+ * couplings, dmrg_setup0). */
+int tsc_create(tsc_ctx** ctx, const tsc_model_config* cfg);
+int tsc_destroy(tsc_ctx* ctx);
+const char* tsc_last_error(tsc_ctx* ctx);
+int tsc_tot_num_up(tsc_ctx* ctx);
+
+/* Uploads one superblock: what model_wave(sys,env,sys_bs,env_bs,...) receives
+ * (get_sys.f90:6915) -- the sys and env Total_Model (ham + boundary operators)
+ * and the enlarged bases -- followed by the Wave layout of psi that fixes the
+ * sector list (Super_Basis, block.f90:2194-2247; its data part is ignored).
+ * Builds hmerge's merged operators (get_sys.f90:7398-7626) and the H.psi task
+ * list on the device. */
+int tsc_superblock_set(tsc_ctx* ctx, int sys_len, int env_len, const int* ints, long long nints,
+                       const double* data, long long ncplx);
+long long tsc_superblock_dim(tsc_ctx* ctx);
+
+/* model_wave (get_sys.f90:6915-7393): out = H in, host complex128 buffers of
+ * tsc_superblock_dim() elements (host->device and device->host copies included). */
+int tsc_hpsi(tsc_ctx* ctx, const double* in, double* out);
+/* Same on device pointers, enqueued on the context stream (no host copies). */
+int tsc_hpsi_device(tsc_ctx* ctx, const void* d_in, void* d_out);
+
+/* lanczos_memo_new (eigen.f90:4-199, levels=1): psi_inout is the start vector
+ * on entry and the normalised ground state on exit (host buffer). */
+int tsc_lanczos(tsc_ctx* ctx, double* psi_inout, double lanzero, int* iters, double* e0);
+
+/* Get_density_matrix_{sys,env}_new + Get_truncation_operator (den_mat.f90:4-418)
+ * on the ground state psi (host buffer).  side 0 = sys, 1 = env.  Writes the
+ * kept count, discarded weight, entropies; the truncation operator U in the Block
+ * layout is returned through *trun_ints / *trun_data (library-owned, valid until
+ * the next call on ctx). spectrum (may be NULL) receives the sorted normalised
+ * density-matrix spectrum (up to spectrum_cap entries). */
+int tsc_truncate(tsc_ctx* ctx, int side, const double* psi, int kept_min, int kept_max,
+                 double trun_err, int* num_state, double* err, double* entropy,
+                 double* entropy_mult, const int** trun_ints, long long* ntrun_ints,
+                 const double** trun_data, long long* ntrun_cplx, double* spectrum,
+                 long long spectrum_cap);
+
+/* Get_Hamiltonian_Sys / Get_Hamiltonian_Env (get_sys.f90:4-592): enlarges the
+ * block of the given side with one site (update_block_*, update_site_*,
+ * Get_hamiltonian_*) and renormalises every operator with U (update_trun_dia /
+ * update_trun_ndia, block.f90:3465-3683).  Inputs: the Model, the enlarged Basis
+ * and the truncation Block.  mshift is the reference's mshift for the env side.
+ * The grown Model is returned through *out_ints / *out_data (library-owned). */
+int tsc_renormalize(tsc_ctx* ctx, int side, int sys_len, int env_len, int mshift,
+                    const int* ints, long long nints, const double* data, long long ncplx,
+                    const int** out_ints, long long* nout_ints, const double** out_data,
+                    long long* nout_cplx);
+
+/* wave_trans_LR / wave_trans_RL (dmrg_sub.f90:1471-1789): dir 0 = LR, 1 = RL.
+ * ints/data: sys Basis, env Basis, sys truncation Block, env truncation Block,
+ * old Wave, new Wave layout (data ignored).  new_out receives the new wave. */
+int tsc_wave_transform(tsc_ctx* ctx, int dir, const int* ints, long long nints, const double* data,
+                       long long ncplx, double* new_out);
+
+/* Whole ground-state search on the device (Get_Ground_State, main.f90:114-209):
+ * warm-up, two half sweeps and nsweeps full sweeps, blocks resident in HBM.
+ * Writes up to max_steps records; returns the number of Lanczos solves. */
+int tsc_dmrg_run(tsc_ctx* ctx, const tsc_sweep_config* sweep, tsc_step_log* log, int max_steps);
+
+/* Serialises the superblock of the most recent step of tsc_dmrg_run whose
+ * global solve index equals capture_step (set before the run with
+ * tsc_set_capture); layout = tsc_superblock_set input with psi data. */
+int tsc_set_capture(tsc_ctx* ctx, int capture_step);
+int tsc_get_capture(tsc_ctx* ctx, const int** ints, long long* nints, const double** data,
+                    long long* ncplx, int* sys_len, int* env_len);
+
+/* Timing of the last tsc_hpsi / tsc_hpsi_device: device milliseconds of its
+ * grouped-GEMM launches (CUDA events on the context stream), the algorithmic
+ * flops of one model_wave in the reference's GEMM association order, the flops
+ * the kernels execute (fewer: shared left products), and the launch count. */
+int tsc_hpsi_stats(tsc_ctx* ctx, double* device_ms, double* ref_flops, double* exec_flops, int* launches);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* TSC_GPU_H */

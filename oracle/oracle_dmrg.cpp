@@ -358,6 +358,62 @@ void update_trun_ndia(const Block& ori, Block& eff, const Block& trun) {
   }
 }
 
+// Density-matrix eigenvalues below this are rounding noise (rho has unit trace).
+const double kZeroWeight = 1e-13;
+
+// Canonical orthonormal basis of the complement of span(Q) (d x s): Gram-Schmidt
+// of the unit vectors e_0, e_1, ... in order, keeping candidates whose projected
+// norm exceeds a threshold.  Depends on Q only through its projector, so every
+// eigensolver yields the same kept zero-weight states.  Not in the reference
+// (den_mat.f90:395-396 keeps whatever null vectors its LAPACK returns).
+void null_completion(int d, int s, const cplx* Q, int m, cplx* N) {
+  int got = 0;
+  std::vector<cplx> v(d);
+  for (double thr : {0.5, 0.1, 1e-3}) {
+    for (int j = 0; j < d && got < m; ++j) {
+      std::fill(v.begin(), v.end(), cplx(0.0));
+      v[j] = 1.0;
+      for (int pass = 0; pass < 2; ++pass) {
+        for (int q = 0; q < s; ++q) {
+          cplx dot = 0.0;
+          for (int r = 0; r < d; ++r) dot += std::conj(Q[(size_t)q * d + r]) * v[r];
+          for (int r = 0; r < d; ++r) v[r] -= dot * Q[(size_t)q * d + r];
+        }
+        for (int q = 0; q < got; ++q) {
+          cplx dot = 0.0;
+          for (int r = 0; r < d; ++r) dot += std::conj(N[(size_t)q * d + r]) * v[r];
+          for (int r = 0; r < d; ++r) v[r] -= dot * N[(size_t)q * d + r];
+        }
+      }
+      double nrm = 0.0;
+      for (int r = 0; r < d; ++r) nrm += std::norm(v[r]);
+      nrm = std::sqrt(nrm);
+      if (nrm <= thr) continue;
+      for (int r = 0; r < d; ++r) N[(size_t)got * d + r] = v[r] / nrm;
+      got++;
+    }
+    if (got >= m) return;
+  }
+  throw std::runtime_error("null_completion: complement too small");
+}
+
+// Canonical phase of every eigenvector column: multiply by conj(z)/|z| with
+// z = sum_r w_r u_r, w_r = 1/(1 + r/10).  Eigensolvers return eigenvectors with
+// arbitrary phases (the reference inherits MKL's); fixing them makes the
+// renormalised operators, and therefore a random start vector's meaning,
+// independent of the eigensolver.  Not in the reference.
+void phase_fix(int rows, int cols, cplx* U) {
+  for (int c = 0; c < cols; ++c) {
+    cplx* u = U + (size_t)c * rows;
+    cplx z = 0.0;
+    for (int r = 0; r < rows; ++r) z += u[r] * (1.0 / (1.0 + 0.1 * r));
+    double a = std::abs(z);
+    if (a < 1e-10) continue;
+    cplx f = std::conj(z) / a;
+    for (int r = 0; r < rows; ++r) u[r] *= f;
+  }
+}
+
 // QuickSort_Double, block.f90:2398-2444 (descending, carries an index array)
 void quicksort_double(std::vector<double>& arr, std::vector<int>& idx, int lower, int upper) {
   int i = lower, j = upper;
@@ -562,6 +618,10 @@ void Oracle::truncation_operator(const Block& den, Block& trun, double trun_err,
       scipy_zheev_(&jobz, &uplo, &n, evec[k].data(), &lda, eval[k].data(), work.data(), &lwork,
                    rwork.data(), &info);
     }
+    phase_fix(n, n, evec[k].data());
+    // eigenvalues at rounding-noise level count as exact zeros (see null_completion)
+    for (int i = 0; i < n; ++i)
+      if (eval[k][i] < kZeroWeight) eval[k][i] = 0.0;
     for (int i = 0; i < n; ++i) sidx[k][i] = dim + i + 1;
     dim += n;
   }
@@ -626,6 +686,16 @@ void Oracle::truncation_operator(const Block& den, Block& trun, double trun_err,
     int row = s.row_dim, col = s.sdim;
     for (int c = 0; c < col; ++c)
       for (int r = 0; r < row; ++r) s.at(r, c) = evec[i][(size_t)(row - col + c) * row + r];
+    // kept columns of zero weight: canonical null-space basis instead of the
+    // eigensolver's arbitrary vectors (columns stay in ascending-weight order)
+    int sig = 0;
+    for (int c = 0; c < col; ++c)
+      if (eval[i][row - col + c] > 0.0) sig++;
+    if (sig < col) {
+      std::vector<cplx> nul((size_t)row * (col - sig));
+      null_completion(row, sig, &s.mat[(size_t)(col - sig) * row], col - sig, nul.data());
+      std::copy(nul.begin(), nul.end(), s.mat.begin());
+    }
     trun.sub.push_back(std::move(s));
   }
   trun.num = (int)trun.sub.size();

@@ -1,0 +1,271 @@
+// Host side of the B200 superblock engine: device-resident block operators,
+// SU(2) bases, task-list builders for the grouped-GEMM kernel, the Lanczos /
+// truncation / renormalisation / wave-transformation steps and the sweep driver.
+// Sector conventions follow the reference data model (DMRG_code/common.f90:84-156):
+// a sector is (num_up, num_down) = (electrons, 2S); operator sub-blocks are keyed
+// by their column sector and carry their own down_dif; matrices hold reduced
+// (Wigner-Eckart) elements.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <array>
+#include <complex>
+#include <map>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "tsc_kernels.cuh"
+
+namespace tsc {
+
+using cplx = std::complex<double>;
+
+struct Error : std::runtime_error {
+  int code;
+  Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+void cuda_check(cudaError_t e, const char* what);
+
+// ---- device memory -----------------------------------------------------------
+struct DevBuf {
+  double2* p = nullptr;
+  size_t n = 0;   // complex elements
+  cudaStream_t st = nullptr;
+  DevBuf() = default;
+  DevBuf(size_t count, cudaStream_t s, bool zero);
+  ~DevBuf();
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+};
+using DevBufP = std::shared_ptr<DevBuf>;
+
+// ---- data model ----------------------------------------------------------------
+struct SubDesc {
+  int num_up = 0, num_down = 0, down_dif = 0, row_dim = 0, sdim = 0;
+  long long off = 0;   // complex elements from the block's buffer start
+};
+struct DBlock {
+  int len = 0, num = 0, dim = 0, up_dif = 0, down_dif = 0;
+  std::vector<SubDesc> sub;
+  DevBufP buf;
+  double2* ptr(int i) const { return buf->p + sub[i].off; }
+  long long total() const {
+    long long t = 0;
+    for (auto& s : sub) t += (long long)s.row_dim * s.sdim;
+    return t;
+  }
+};
+enum OpIdx { OP_UP = 0, OP_DOWN = 1, OP_SD = 2, OP_SN = 3 };
+struct OpSet {
+  DBlock op[4];
+};
+struct DModel {
+  int len = 0;
+  DBlock ham;
+  std::vector<OpSet> sub;   // 1-based boundary-site operators
+};
+struct Piece {
+  int spos = 0, sdim = 0, bl_num_up = 0, bl_num_down = 0, st_num_up = 0, st_num_down = 0;
+};
+struct Sector {
+  int num_up = 0, num_down = 0, dim = 0;
+  std::vector<Piece> pcs;
+};
+struct Basis {
+  int len = 0, num = 0, dim = 0;
+  std::vector<Sector> sec;
+  int find(int up, int down) const {
+    for (int x = 0; x < num; ++x)
+      if (sec[x].num_up == up && sec[x].num_down == down) return x;
+    return -1;
+  }
+};
+struct WSec {
+  int sys_num_up = 0, sys_num_down = 0, env_num_up = 0, env_num_down = 0, sys_dim = 0, env_dim = 0;
+  long long off = 0;
+};
+struct WLayout {
+  int sys_len = 0, env_len = 0, num = 0;
+  long long dim = 0;
+  std::vector<WSec> sec;
+  int find(int su, int sd, int eu, int ed) const {
+    for (int k = 0; k < num; ++k) {
+      const WSec& s = sec[k];
+      if (s.sys_num_up == su && s.sys_num_down == sd && s.env_num_up == eu && s.env_num_down == ed) return k;
+    }
+    return -1;
+  }
+};
+
+// site operators (dmrg_sub.f90:733-908) held on the host: one 1x1 element per sub-block
+struct SiteSub {
+  int num_up, num_down, down_dif;
+  double val;
+};
+struct SiteOp {
+  int up_dif = 0, down_dif = 0;
+  std::vector<SiteSub> sub;
+};
+
+// ---- lattice and couplings (dmrg_sub.f90:304-644, main.f90:59-99) ----------------
+struct Lattice {
+  int Nx = 0, Ny = 0, nleg = 0, num_site = 0, openy = 0;
+  static constexpr int neibt = 18;
+  std::vector<int> neib, neiba, nposi, nposi_dm, nposi_lat, inb1, nleg11, inb;
+  std::vector<double> jt, jz, jd, jn;
+  int nxc = 0;
+  int coup_bs[2][2] = {{0, 0}, {0, 0}}, coup_bb[2] = {0, 0};
+  void init(int Nx, int Ny, double t1, double t2, double J1, double J2, int openy);
+  void setup(int ns, int ns21);   // dmrg_setup
+  void setup0();                  // dmrg_setup0
+  int& NEIB(int i, int k) { return neib[(size_t)i * (neibt + 1) + k]; }
+  int& NEIBA(int i, int j) { return neiba[(size_t)i * (num_site + 1) + j]; }
+  int& INB1(int i, int ns) { return inb1[(size_t)i * (num_site + 1) + ns]; }
+  int& INB(int i) { return inb[(size_t)(i + 4)]; }
+  double JT(int k, int s) const { return jt[(size_t)s * (neibt + 1) + k]; }
+  double JZ(int k, int s) const { return jz[(size_t)s * (neibt + 1) + k]; }
+  double JD(int k, int s) const { return jd[(size_t)s * (neibt + 1) + k]; }
+  double JN(int k, int s) const { return jn[(size_t)s * (neibt + 1) + k]; }
+  int npos(int latt) const { return nposi[nposi_dm[latt]]; }
+};
+
+double w6j(int j1, int j2, int j3, int l1, int l2, int l3);   // doubled arguments
+
+// ---- task lists -------------------------------------------------------------------
+struct TaskList {
+  std::vector<GGroup> groups;
+  std::vector<std::vector<GTerm>> gterms;   // per-group terms while building
+  // device copies
+  DevBufP dev;   // jobs + groups + terms packed (as raw bytes in a double2 buffer)
+  GJob* d_jobs = nullptr;
+  GGroup* d_groups = nullptr;
+  GTerm* d_terms = nullptr;
+  int njobs = 0;
+  double exec_flops = 0;   // flops the kernel executes
+  long long nterms = 0;
+  int add_group(double2* abs_c, uint8_t base, long long c_off, int ld, int M, int N, int beta);
+  void upload(cudaStream_t st);
+};
+
+struct Stats {
+  double hpsi_ms = 0, hpsi_flops = 0, hpsi_bytes = 0;
+  int launches = 0;
+};
+
+class Engine {
+ public:
+  Engine(int Nx, int Ny, double t1, double t2, double J1, double J2, int delta, int device);
+  ~Engine();
+
+  cudaStream_t st = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  Lattice L;
+  int tot_num_up = 0, tot_num_down = 0;
+  SiteOp st_elec_up, st_elec_down, num_elec, st_sd, st_sz;
+  std::string last_error;
+
+  // ---- superblock (one Lanczos problem) ----
+  struct Superblock {
+    DModel sys, env;
+    Basis sys_bs, env_bs;
+    WLayout wl;
+    DBlock snc_sys[2][4], snc_env[2][4];
+    std::vector<OpSet> sub_s_sys, sub_s_env;   // merged block-block operators
+    TaskList merge;            // hmerge axpy tasks
+    TaskList p1, p2;           // H.psi phase 1 (intermediates) and phase 2 (outputs)
+    long long scratch_elems = 0;
+    DevBufP scratch;
+    double ref_flops = 0;      // algorithmic flops of one model_wave (reference order)
+    bool valid = false;
+  } sb;
+
+  void superblock_set(DModel&& sys, DModel&& env, Basis&& sys_bs, Basis&& env_bs, WLayout&& wl);
+  void hpsi(const double2* d_in, double2* d_out);   // enqueue on st
+  Stats last_stats;
+
+  // Lanczos (eigen.f90:4-199) on the current superblock; psi device buffer in/out
+  void lanczos(double2* d_psi, double lanzero, int* iters, double* e0, double* hpsi_ms, int* hpsi_calls);
+
+  // density matrix + truncation (den_mat.f90)
+  struct TruncResult {
+    DBlock trun;
+    int num_state = 0;
+    double err = 0, ent = 0, ent_mult = 0;
+    std::vector<double> spectrum;
+  };
+  void truncate(int side, const double2* d_psi, const WLayout& wl, int kept_min, int kept_max,
+                double trun_err, TruncResult& out);
+
+  // block growth + renormalisation (get_sys.f90:4-592)
+  void grow(int side, DModel& pre, const Basis& basis, const DBlock& trun, int mshift);
+
+  // wave transformations (dmrg_sub.f90:1471-1789); new_w zeroed and written
+  void wave_trans(int dir, const Basis& sys_bs, const Basis& env_bs, const DBlock& sys_trun,
+                  const DBlock& env_trun, const WLayout& old_l, const double2* d_old, const WLayout& new_l,
+                  double2* d_new);
+
+  // bases (block.f90:2087-2247)
+  Basis get_basis(const DBlock& block) const;
+  WLayout get_super(const Basis& sys_bs, const Basis& env_bs, int tot_up, int tot_down) const;
+  DModel site_model() const;
+
+  // sweep driver (dmrg_sub.f90:974-1465, main.f90:114-209)
+  struct StepRec {
+    int phase, sys_len, env_len;
+    double e0;
+    int iters, num_state;
+    double err, ent, ent_mult;
+    int hpsi_calls;
+    double hpsi_seconds, hpsi_flops, step_seconds;
+  };
+  void run(int kept_min, int kept_warm, const std::vector<int>& sweeps, double lanzero_override,
+           unsigned long long seed, std::vector<StepRec>* log);
+  int capture_step = -1;
+  struct Capture {
+    bool valid = false;
+    std::vector<int> ints;
+    std::vector<cplx> data;
+    int sys_len = 0, env_len = 0;
+  } cap;
+
+  // helpers
+  void normalize(double2* d, long long n);
+  double wave_norm2(const double2* d, long long n);
+  DBlock upload_block(const int*& ip, const cplx*& dp);
+  void download_block(const DBlock& b, std::vector<int>& ints, std::vector<cplx>& data) const;
+  DBlock copy_block(const DBlock& b);
+
+  // scratch for reductions
+  DevBufP red_buf;
+  double* d_red = nullptr;   // partials
+  double* d_scal = nullptr;  // scalars: [0..255] alpha, [256..511] beta, [512..767] uv, [768..1023] uu, misc
+  double* h_scal = nullptr;  // pinned mirror
+
+ private:
+  uint64_t rng = 1;
+  double rand01();
+  void wave_initialize(const WLayout& wl, double2* d);
+  std::map<int, DModel> sys_models, env_models;
+  std::map<int, DBlock> sys_truns, env_truns;
+  std::map<int, Basis> sys_bsm, env_bsm;
+  WLayout disk_layout;
+  DevBufP disk_wave;
+  int restart1 = 0;
+  int kept_min_ = 0, kept_max_ = 0;
+  double lanzero_ = 0;
+  int nsolve_ = 0;
+  void lanczos_step(int phase, DModel& sys, DModel& env, const Basis& sys_bs, const Basis& env_bs,
+                    const WLayout& wl, DevBufP& psi, StepRec& rec);
+  void build_hpsi_tasks();
+  void build_merge();
+  void run_tasks(TaskList& tl, double2* in, double2* out, double2* scr);
+  void capture_superblock(const DevBufP& psi);
+  void warm_up(int end_id, double trun_err, std::vector<StepRec>* log);
+  void left_to_right(int bg_id, int end_id, double trun_err, std::vector<StepRec>* log);
+  void right_to_left(int bg_id, int end_id, double trun_err, std::vector<StepRec>* log);
+};
+
+}  // namespace tsc

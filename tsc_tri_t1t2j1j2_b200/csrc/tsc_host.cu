@@ -1,0 +1,505 @@
+// Host set-up of the engine: device memory, lattice tables, SU(2) 6j symbols,
+// site operators, bases and task-list packing.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "tsc_engine.hpp"
+
+namespace tsc {
+
+void cuda_check(cudaError_t e, const char* what) {
+  if (e != cudaSuccess) throw Error(e == cudaErrorMemoryAllocation ? -5 : -3,
+                                    std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+DevBuf::DevBuf(size_t count, cudaStream_t s, bool zero) : n(count), st(s) {
+  if (count == 0) return;
+  cuda_check(cudaMallocAsync((void**)&p, count * sizeof(double2), s), "cudaMallocAsync");
+  if (zero) cuda_check(cudaMemsetAsync(p, 0, count * sizeof(double2), s), "cudaMemsetAsync");
+}
+DevBuf::~DevBuf() {
+  if (p) cudaFreeAsync(p, st);
+}
+
+// ---- SU(2) coefficients --------------------------------------------------------
+// Racah's closed form for the 6j symbol with doubled arguments (the reference's
+// W6JS, block.f90:3744-3795, evaluates the same sum with a table of factorials).
+static double g_fact[171];
+static bool g_fact_ready = false;
+static void fact_init() {
+  if (g_fact_ready) return;
+  g_fact[0] = 1.0;
+  for (int i = 1; i <= 170; ++i) g_fact[i] = g_fact[i - 1] * (double)(float)i;
+  g_fact_ready = true;
+}
+
+double w6j(int j1, int j2, int j3, int l1, int l2, int l3) {
+  fact_init();
+  // triangle (j1 j2 j3), (j1 l2 l3), (l1 j2 l3), (l1 l2 j3) with integer sums
+  auto tri = [](int a, int b, int c) { return c <= a + b && c >= std::abs(a - b) && ((a + b + c) & 1) == 0; };
+  if (!tri(j1, j2, j3) || !tri(j1, l2, l3) || !tri(l1, j2, l3) || !tri(l1, l2, j3)) return 0.0;
+  const int s1 = j1 + j2 + j3, s2 = j1 + l2 + l3, s3 = l1 + j2 + l3, s4 = l1 + l2 + j3;
+  const int p1 = j1 + j2 + l1 + l2, p2 = j2 + j3 + l2 + l3, p3 = j3 + j1 + l3 + l1;
+  const int wlo = std::max(std::max(s1, s2), std::max(s3, s4));
+  const int whi = std::min(p1, std::min(p2, p3));
+  double omega = 0.0;
+  for (int w = wlo; w <= whi; w += 2) {
+    double den = g_fact[(w - s1) / 2] * g_fact[(w - s2) / 2] * g_fact[(w - s3) / 2] * g_fact[(w - s4) / 2] *
+                 g_fact[(p1 - w) / 2] * g_fact[(p2 - w) / 2] * g_fact[(p3 - w) / 2];
+    if (w % 4 != 0) den = -den;
+    omega = omega + g_fact[w / 2 + 1] / den;
+  }
+  auto delta = [](int a, int b, int c) {
+    return g_fact[(a + b - c) / 2] * g_fact[(a - b + c) / 2] * g_fact[(-a + b + c) / 2] / g_fact[(a + b + c) / 2 + 1];
+  };
+  double th = delta(j1, j2, j3) * delta(j1, l2, l3) * delta(l1, j2, l3) * delta(l1, l2, j3);
+  return omega * std::sqrt(th);
+}
+
+// ---- lattice (dmrg_sub.f90:304-644) -------------------------------------------------
+void Lattice::init(int nx, int ny, double t1, double t2, double J1, double J2, int oy) {
+  Nx = nx;
+  Ny = ny;
+  nleg = ny;
+  num_site = nx * ny;
+  openy = oy;
+  int N = num_site;
+  neib.assign((size_t)(N + 1) * (neibt + 1), 0);
+  neiba.assign((size_t)(N + 1) * (N + 1), 0);
+  nposi.assign(N + 8, 0);
+  nposi_dm.assign(N + 8, 0);
+  nposi_lat.assign(N + 8, 0);
+  inb1.assign((size_t)(N + 1) * (N + 1), 0);
+  nleg11.assign(N + 1, 0);
+  inb.assign(N + 8, 0);
+  size_t nc = (size_t)(N + 1) * (neibt + 1);
+  jt.assign(nc, 0.0);
+  jz.assign(nc, 0.0);
+  jd.assign(nc, 0.0);
+  jn.assign(nc, 0.0);
+  for (int s = 1; s <= N; ++s) {
+    for (int k = 1; k <= 12; ++k) {
+      size_t e = (size_t)s * (neibt + 1) + k;
+      jz[e] = k <= 6 ? J1 : J2;
+      jt[e] = -(k <= 6 ? t1 : t2) * std::sqrt(2.0);
+      jn[e] = -0.25 * jz[e];
+    }
+    for (int k = 1; k <= 18; ++k) {
+      size_t e = (size_t)s * (neibt + 1) + k;
+      jd[e] = jz[e] * (-std::sqrt(3.0));
+    }
+  }
+}
+
+void Lattice::setup(int ns, int ns21) {
+  int nn = ns + ns21 + 2;
+  nxc = (nn - 1) / nleg + 1;
+  if (nxc == 1) nxc = 2;
+  std::fill(nposi.begin(), nposi.end(), 0);
+  std::fill(nposi_dm.begin(), nposi_dm.end(), 0);
+  std::fill(nposi_lat.begin(), nposi_lat.end(), 0);
+  std::fill(neib.begin(), neib.end(), 0);
+  std::fill(neiba.begin(), neiba.end(), 0);
+  int totsite = nleg * nxc;
+  for (int i = 1; i <= ns + 1; ++i) {
+    nposi[i] = 1;
+    nposi_lat[i] = i;
+    nposi_dm[i] = i;
+  }
+  nposi[ns + 1] = 2;
+  for (int i = 1; i <= ns21 + 1; ++i) {
+    nposi[ns + 1 + i] = 3;
+    nposi_dm[totsite + 1 - i] = i + ns + 1;
+    nposi_lat[i + ns + 1] = totsite + 1 - i;
+  }
+  nposi[ns + ns21 + 2] = 4;
+  auto link = [&](int a, int ka, int b, int kb) {
+    NEIB(a, ka) = b;
+    NEIB(b, kb) = a;
+    NEIBA(a, b) = ka;
+    NEIBA(b, a) = kb;
+  };
+  for (int ix = 1; ix <= nxc; ++ix)
+    for (int iy = 1; iy <= nleg; ++iy) {
+      int ii = iy + (ix - 1) * nleg;
+      int jy = ii - iy + (iy % nleg) + 1;
+      if (openy != 0 && iy == nleg) jy = 0;
+      if (jy != 0 && (iy != nleg || nleg != 2)) link(ii, 1, jy, 2);
+      int jx = ii + nleg;
+      if (jx > nleg * nxc) jx = 0;   // open in x
+      if (jx != 0) {
+        link(ii, 3, jx, 4);
+        jy = jx - 1;
+        if (iy == 1) jy = openy == 0 ? jy + nleg : 0;
+        if (jy != 0) link(ii, 5, jy, 6);
+      }
+    }
+  for (int ix = 1; ix <= nxc; ++ix)
+    for (int iy = 1; iy <= nleg; ++iy) {
+      int ii = iy + (ix - 1) * nleg;
+      int a = NEIB(ii, 1), b = NEIB(a, 3);
+      if (a * b != 0) link(ii, 7, b, 8);
+      if (nleg != 3) {
+        a = NEIB(ii, 3);
+        b = NEIB(a, 5);
+        if (a * b != 0) link(ii, 9, b, 10);
+      }
+      a = NEIB(ii, 2);
+      b = NEIB(a, 5);
+      if (a * b != 0) link(ii, 11, b, 12);
+      if (nleg != 3) {
+        a = NEIB(ii, 1);
+        b = NEIB(a, 1);
+        if (a * b != 0 && NEIBA(ii, b) == 0) link(ii, 13, b, 14);
+      }
+      a = NEIB(ii, 3);
+      b = NEIB(a, 3);
+      if (a * b != 0 && NEIBA(ii, b) == 0) link(ii, 15, b, 16);
+      a = NEIB(ii, 5);
+      b = NEIB(a, 5);
+      if (a * b != 0 && NEIBA(ii, b) == 0) link(ii, 17, b, 18);
+    }
+  for (int i = 1; i <= num_site; ++i)
+    for (int j = 7; j <= neibt; ++j)
+      if (std::fabs(JZ(j, 1)) + std::fabs(JD(j, 1)) + std::fabs(JT(j, 1)) + std::fabs(JN(j, 1)) == 0.0) {
+        int nb = NEIB(i, j);
+        NEIBA(i, nb) = 0;
+        NEIBA(nb, i) = 0;
+        NEIB(i, j) = 0;
+      }
+}
+
+void Lattice::setup0() {
+  std::fill(nleg11.begin(), nleg11.end(), 0);
+  for (int ns = 1; ns <= num_site - 2; ++ns) {
+    int k0 = 0;
+    for (int i1 = 1; i1 <= ns; ++i1) {
+      int cnt = 0;
+      for (int j = 1; j <= neibt; ++j)
+        if (NEIB(i1, j) >= ns) cnt++;
+      INB1(i1, ns) = cnt ? ++k0 : 10000;
+    }
+    nleg11[ns] = k0;
+  }
+}
+
+// ---- engine -------------------------------------------------------------------------
+Engine::Engine(int Nx, int Ny, double t1, double t2, double J1, double J2, int delta, int device) {
+  if (Nx < 2 || Ny < 2 || Nx * Ny > 1024) throw Error(-1, "lattice size out of range");
+  if (delta < 1) throw Error(-1, "delta must be >= 1");
+  int ndev = 0;
+  cuda_check(cudaGetDeviceCount(&ndev), "cudaGetDeviceCount");
+  if (device < 0 || device >= ndev) throw Error(-1, "no such CUDA device");
+  cuda_check(cudaSetDevice(device), "cudaSetDevice");
+  cuda_check(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "cudaStreamCreate");
+  cuda_check(cudaEventCreate(&ev0), "cudaEventCreate");
+  cuda_check(cudaEventCreate(&ev1), "cudaEventCreate");
+  L.init(Nx, Ny, t1, t2, J1, J2, 0);
+  // site operators (dmrg_sub.f90:743-906)
+  st_elec_up.up_dif = 1;
+  st_elec_up.down_dif = 1;
+  st_elec_up.sub = {{0, 0, 1, -std::sqrt(2.0)}};
+  st_elec_down.up_dif = -1;
+  st_elec_down.down_dif = 1;
+  st_elec_down.sub = {{1, 1, -1, -std::sqrt(2.0)}};
+  num_elec.sub = {{1, 1, 0, std::sqrt(2.0)}, {0, 0, 0, 0.0}};
+  st_sd.down_dif = 2;
+  st_sd.sub = {{1, 1, 0, std::sqrt(1.5)}};
+  st_sz.sub = {{1, 1, 0, 1.0}, {0, 0, 0, 0.0}};
+  int N = L.num_site;
+  tot_num_up = 2 * (N / 2 - (N + 2 * delta - 1) / (2 * delta));
+  tot_num_down = 0;
+  L.setup(N / 2 - 1, N / 2 - 1);
+  L.setup0();
+  red_buf = std::make_shared<DevBuf>((size_t)(1 << 16) + 1024, st, true);
+  d_red = reinterpret_cast<double*>(red_buf->p);
+  d_scal = d_red + (1 << 16);
+  cuda_check(cudaMallocHost((void**)&h_scal, 2048 * sizeof(double)), "cudaMallocHost");
+}
+
+Engine::~Engine() {
+  sb = Superblock();
+  sys_models.clear();
+  env_models.clear();
+  sys_truns.clear();
+  env_truns.clear();
+  disk_wave.reset();
+  red_buf.reset();
+  if (st) cudaStreamSynchronize(st);
+  if (h_scal) cudaFreeHost(h_scal);
+  if (ev0) cudaEventDestroy(ev0);
+  if (ev1) cudaEventDestroy(ev1);
+  if (st) cudaStreamDestroy(st);
+}
+
+DModel Engine::site_model() const {   // Get_hamiltonian_site, dmrg_sub.f90:912-938
+  DModel m;
+  m.len = 1;
+  auto mk = [&](const SiteOp& so, int nsub_override_zero) {
+    DBlock b;
+    b.len = 1;
+    b.num = (int)so.sub.size();
+    b.dim = b.num;
+    b.up_dif = so.up_dif;
+    b.down_dif = so.down_dif;
+    b.buf = std::make_shared<DevBuf>((size_t)b.num, st, false);
+    std::vector<double2> h(b.num);
+    for (int i = 0; i < b.num; ++i) {
+      SubDesc s;
+      s.num_up = so.sub[i].num_up;
+      s.num_down = so.sub[i].num_down;
+      s.down_dif = so.sub[i].down_dif;
+      s.row_dim = s.sdim = 1;
+      s.off = i;
+      b.sub.push_back(s);
+      h[i] = make_double2(nsub_override_zero ? 0.0 : so.sub[i].val, 0.0);
+    }
+    cuda_check(cudaMemcpyAsync(b.buf->p, h.data(), b.num * sizeof(double2), cudaMemcpyHostToDevice, st), "upload");
+    cuda_check(cudaStreamSynchronize(st), "sync");
+    return b;
+  };
+  m.ham = mk(st_sz, 1);
+  m.sub.resize(L.num_site + 1);
+  m.sub[1].op[OP_UP] = mk(st_elec_up, 0);
+  m.sub[1].op[OP_DOWN] = mk(st_elec_down, 0);
+  m.sub[1].op[OP_SD] = mk(st_sd, 0);
+  m.sub[1].op[OP_SN] = mk(num_elec, 0);
+  return m;
+}
+
+// Get_basis, block.f90:2087-2188 (site = st_sz: (1,1) then (0,0), sdim 1)
+Basis Engine::get_basis(const DBlock& block) const {
+  Basis b;
+  b.len = block.len + 1;
+  std::vector<std::pair<int, int>> q;   // (N, 2S)
+  for (const auto& s : block.sub)
+    for (const auto& t : st_sz.sub)
+      for (int ss = std::abs(s.num_down - t.num_down); ss <= s.num_down + t.num_down; ss += 2)
+        q.push_back({s.num_up + t.num_up, ss});
+  // descending 2S, then descending N (QuickSort_Integer, block.f90:2316-2349), unique
+  std::sort(q.begin(), q.end(), [](const std::pair<int, int>& a, const std::pair<int, int>& c) {
+    if (a.second != c.second) return a.second > c.second;
+    return a.first > c.first;
+  });
+  q.erase(std::unique(q.begin(), q.end()), q.end());
+  b.num = (int)q.size();
+  b.sec.resize(b.num);
+  for (int i = 0; i < b.num; ++i) {
+    Sector& S = b.sec[i];
+    S.num_up = q[i].first;
+    S.num_down = q[i].second;
+    for (const auto& s : block.sub)
+      for (const auto& t : st_sz.sub) {
+        if (s.num_up + t.num_up != S.num_up) continue;
+        if (S.num_down < std::abs(s.num_down - t.num_down) || S.num_down > s.num_down + t.num_down) continue;
+        Piece p;
+        p.bl_num_up = s.num_up;
+        p.bl_num_down = s.num_down;
+        p.st_num_up = t.num_up;
+        p.st_num_down = t.num_down;
+        p.sdim = s.sdim;
+        p.spos = S.dim;
+        S.dim += p.sdim;
+        S.pcs.push_back(p);
+      }
+    b.dim += S.dim;
+  }
+  return b;
+}
+
+// Get_super_basis, block.f90:2194-2247
+WLayout Engine::get_super(const Basis& sys_bs, const Basis& env_bs, int tot_up, int tot_down) const {
+  WLayout w;
+  w.sys_len = sys_bs.len;
+  w.env_len = env_bs.len;
+  for (const auto& s : sys_bs.sec)
+    for (const auto& e : env_bs.sec) {
+      if (e.num_up != tot_up - s.num_up) continue;
+      if (tot_down < std::abs(e.num_down - s.num_down) || tot_down > e.num_down + s.num_down) continue;
+      WSec x;
+      x.sys_num_up = s.num_up;
+      x.sys_num_down = s.num_down;
+      x.env_num_up = e.num_up;
+      x.env_num_down = e.num_down;
+      x.sys_dim = s.dim;
+      x.env_dim = e.dim;
+      x.off = w.dim;
+      w.dim += (long long)s.dim * e.dim;
+      w.sec.push_back(x);
+    }
+  w.num = (int)w.sec.size();
+  return w;
+}
+
+// ---- task lists ------------------------------------------------------------------------
+int TaskList::add_group(double2* abs_c, uint8_t base, long long c_off, int ld, int M, int N, int beta) {
+  GGroup g{};
+  g.c_base = base;
+  g.c_off = base == BASE_ABS ? (long long)((uintptr_t)abs_c / sizeof(double2)) + c_off : c_off;
+  g.c_ld = ld;
+  g.M = M;
+  g.N = N;
+  g.beta = (uint8_t)beta;
+  groups.push_back(g);
+  gterms.emplace_back();
+  return (int)groups.size() - 1;
+}
+
+void TaskList::upload(cudaStream_t st) {
+  std::vector<GTerm> terms;
+  std::vector<GJob> jobs;
+  struct JC {
+    GJob j;
+    long long cost;
+  };
+  std::vector<JC> jc;
+  exec_flops = 0;
+  for (size_t gi = 0; gi < groups.size(); ++gi) {
+    GGroup& g = groups[gi];
+    g.t0 = (int)terms.size();
+    long long cost = 1;
+    for (auto& t : gterms[gi]) {
+      terms.push_back(t);
+      if (t.kind == TK_GEMM) {
+        cost += (t.K + GEMM_TK - 1) / GEMM_TK * 4;
+        exec_flops += 8.0 * g.M * g.N * t.K;
+      } else {
+        cost += 1;
+      }
+    }
+    g.t1 = (int)terms.size();
+    if (g.M <= 0 || g.N <= 0) continue;
+    int tm = (g.M + GEMM_TM - 1) / GEMM_TM, tn = (g.N + GEMM_TN - 1) / GEMM_TN;
+    for (int a = 0; a < tm; ++a)
+      for (int b = 0; b < tn; ++b) jc.push_back({GJob{(int)gi, a, b, 0}, cost});
+  }
+  // longest jobs first: the hardware scheduler then approximates LPT balancing
+  std::stable_sort(jc.begin(), jc.end(), [](const JC& a, const JC& b) { return a.cost > b.cost; });
+  for (auto& x : jc) jobs.push_back(x.j);
+  njobs = (int)jobs.size();
+  nterms = (long long)terms.size();
+  size_t bj = jobs.size() * sizeof(GJob), bg = groups.size() * sizeof(GGroup), bt = terms.size() * sizeof(GTerm);
+  auto al = [](size_t x) { return (x + 255) / 256 * 256; };
+  size_t total = al(bj) + al(bg) + al(bt) + 256;
+  dev = std::make_shared<DevBuf>((total + 15) / 16, st, false);
+  char* base = reinterpret_cast<char*>(dev->p);
+  d_jobs = reinterpret_cast<GJob*>(base);
+  d_groups = reinterpret_cast<GGroup*>(base + al(bj));
+  d_terms = reinterpret_cast<GTerm*>(base + al(bj) + al(bg));
+  std::vector<char> host(total, 0);
+  if (bj) std::memcpy(host.data(), jobs.data(), bj);
+  if (bg) std::memcpy(host.data() + al(bj), groups.data(), bg);
+  if (bt) std::memcpy(host.data() + al(bj) + al(bg), terms.data(), bt);
+  cuda_check(cudaMemcpyAsync(base, host.data(), total, cudaMemcpyHostToDevice, st), "task upload");
+  cuda_check(cudaStreamSynchronize(st), "task upload sync");
+  gterms.clear();
+  gterms.shrink_to_fit();
+}
+
+void Engine::run_tasks(TaskList& tl, double2* in, double2* out, double2* scr) {
+  Bases b;
+  b.p[0] = nullptr;
+  b.p[1] = in;
+  b.p[2] = out;
+  b.p[3] = scr;
+  cuda_check(launch_grouped_zgemm(tl.d_jobs, tl.njobs, tl.d_groups, tl.d_terms, b, st), "grouped_zgemm");
+}
+
+// ---- block transfer ----------------------------------------------------------------------
+DBlock Engine::upload_block(const int*& ip, const cplx*& dp) {
+  DBlock b;
+  b.len = *ip++;
+  b.num = *ip++;
+  b.dim = *ip++;
+  b.up_dif = *ip++;
+  b.down_dif = *ip++;
+  if (b.num < 0 || b.num > 1000000) throw Error(-1, "bad block descriptor");
+  long long off = 0;
+  for (int i = 0; i < b.num; ++i) {
+    SubDesc s;
+    s.num_up = *ip++;
+    s.num_down = *ip++;
+    s.down_dif = *ip++;
+    s.row_dim = *ip++;
+    s.sdim = *ip++;
+    if (s.row_dim < 0 || s.sdim < 0) throw Error(-1, "bad sub-block dims");
+    s.off = off;
+    off += (long long)s.row_dim * s.sdim;
+    b.sub.push_back(s);
+  }
+  b.buf = std::make_shared<DevBuf>((size_t)off, st, false);
+  if (off) cuda_check(cudaMemcpyAsync(b.buf->p, dp, off * sizeof(double2), cudaMemcpyHostToDevice, st), "upload");
+  dp += off;
+  return b;
+}
+
+void Engine::download_block(const DBlock& b, std::vector<int>& ints, std::vector<cplx>& data) const {
+  ints.insert(ints.end(), {b.len, b.num, b.dim, b.up_dif, b.down_dif});
+  size_t d0 = data.size();
+  for (const auto& s : b.sub) ints.insert(ints.end(), {s.num_up, s.num_down, s.down_dif, s.row_dim, s.sdim});
+  long long tot = b.total();
+  data.resize(d0 + tot);
+  for (const auto& s : b.sub) {
+    long long n = (long long)s.row_dim * s.sdim;
+    if (n)
+      cuda_check(cudaMemcpyAsync(&data[d0], b.buf->p + s.off, n * sizeof(double2), cudaMemcpyDeviceToHost, st),
+                 "download");
+    d0 += n;
+  }
+  cuda_check(cudaStreamSynchronize(st), "download sync");
+}
+
+DBlock Engine::copy_block(const DBlock& b) {
+  DBlock c = b;
+  long long off = 0;
+  for (auto& s : c.sub) {
+    s.off = off;
+    off += (long long)s.row_dim * s.sdim;
+  }
+  c.buf = std::make_shared<DevBuf>((size_t)off, st, false);
+  for (int i = 0; i < b.num; ++i) {
+    long long n = (long long)b.sub[i].row_dim * b.sub[i].sdim;
+    if (n)
+      cuda_check(cudaMemcpyAsync(c.buf->p + c.sub[i].off, b.buf->p + b.sub[i].off, n * sizeof(double2),
+                                 cudaMemcpyDeviceToDevice, st),
+                 "copy");
+  }
+  return c;
+}
+
+double Engine::wave_norm2(const double2* d, long long n) {
+  cuda_check(launch_multi_dot(d, 0, 1, d, n, d_red, d_scal + 1900, st), "norm");
+  cuda_check(cudaMemcpyAsync(h_scal + 1900, d_scal + 1900, sizeof(double), cudaMemcpyDeviceToHost, st), "d2h");
+  cuda_check(cudaStreamSynchronize(st), "sync");
+  return h_scal[1900];
+}
+
+void Engine::normalize(double2* d, long long n) {
+  if (n <= 0) return;
+  cuda_check(launch_multi_dot(d, 0, 1, d, n, d_red, d_scal + 1901, st), "norm");
+  cuda_check(launch_scale(d, d_scal + 1901, n, 1, st), "scale");
+}
+
+// random_number stand-in (splitmix64 -> uniform [0,1)), block.f90:1154-1180
+double Engine::rand01() {
+  uint64_t z = (rng += 0x9E3779B97F4A7C15ull);
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  z = z ^ (z >> 31);
+  return (double)(z >> 11) * (1.0 / 9007199254740992.0);
+}
+
+void Engine::wave_initialize(const WLayout& wl, double2* d) {
+  std::vector<double2> h((size_t)wl.dim);
+  for (const auto& s : wl.sec) {
+    size_t n = (size_t)s.sys_dim * s.env_dim;
+    for (size_t e = 0; e < n; ++e) h[s.off + e].x = rand01();
+    for (size_t e = 0; e < n; ++e) h[s.off + e].y = rand01();
+  }
+  cuda_check(cudaMemcpyAsync(d, h.data(), h.size() * sizeof(double2), cudaMemcpyHostToDevice, st), "upload");
+  normalize(d, wl.dim);
+  cuda_check(cudaStreamSynchronize(st), "sync");
+}
+
+}  // namespace tsc

@@ -1,0 +1,547 @@
+// B200 (sm_100a) kernels of the superblock engine.
+//
+// grouped_zgemm: output-stationary grouped complex-FP64 GEMM.  Every job is a
+// 64x64 tile of one output group; the CTA sums all terms of the group in
+// registers (DMMA m8n8k4.f64 warp tiles, 4 real MMAs per complex product, alpha
+// folded into the B fragments) and writes the tile once: no atomics, the result
+// does not depend on launch order.  Operand tiles are staged in shared memory by
+// 16-byte cp.async (double buffered, zero fill at the ragged edges); the conj of
+// op(.)=C is applied when fragments are read.  Shared-memory rows are padded by
+// two complex elements so fragment reads are bank-conflict free.
+//
+// Vector kernels: the Lanczos recurrences of eigen.f90:64-94 and the classical
+// Gram-Schmidt of block.f90:1251-1289 as deterministic two-pass reductions, and
+// a tridiagonal lowest-eigenpair solver standing in for LAPACK dstev
+// (eigen.f90:99,117,141): Sturm-sequence bisection for the eigenvalue, inverse
+// iteration with a pivoted tridiagonal LU for the eigenvector.
+#include "tsc_kernels.cuh"
+
+#include <cfloat>
+#include <cmath>
+
+namespace tsc {
+
+namespace {
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem, bool pred) {
+  unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  int sz = pred ? 16 : 0;
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(sz));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
+}
+__device__ __forceinline__ void dmma(double& c0, double& c1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+               : "+d"(c0), "+d"(c1)
+               : "d"(a), "d"(b));
+}
+
+constexpr int TM = GEMM_TM, TN = GEMM_TN, TK = GEMM_TK;
+constexpr int LDS_A = TM + 2, LDS_B = TN + 2;   // complex elements per shared row
+constexpr int STAGE_A = TK * LDS_A, STAGE_B = TK * LDS_B;
+
+struct SmemTiles {
+  double2 a[2][STAGE_A];
+  double2 b[2][STAGE_B];
+};
+
+// Stage op(L)[m0.., k0..] (TM x TK) and op(R)[k0.., n0..] (TK x TN) into shared memory.
+__device__ __forceinline__ void load_tiles(SmemTiles& s, int stage, const GTerm& t, const double2* L,
+                                           const double2* R, int M, int N, int m0, int n0, int k0) {
+  const int tid = threadIdx.x;
+  const int K = t.K;
+  double2* As = s.a[stage];
+  double2* Bs = s.b[stage];
+  if (t.l_op == OP_N) {
+    // L[(m0+i) + (k0+kk)*ld] : contiguous in i
+    const int i = tid & 63;
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+      int kk = (tid >> 6) + 2 * r;
+      bool ok = (m0 + i < M) && (k0 + kk < K);
+      const double2* src = ok ? L + (long long)(m0 + i) + (long long)(k0 + kk) * t.l_ld : L;
+      cp_async16(&As[kk * LDS_A + i], src, ok);
+    }
+  } else {
+    // op(L)[m][k] = conj(L[k + m*ld]) : contiguous in k
+    const int kk = tid & 15;
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+      int i = (tid >> 4) + 8 * r;
+      bool ok = (m0 + i < M) && (k0 + kk < K);
+      const double2* src = ok ? L + (long long)(k0 + kk) + (long long)(m0 + i) * t.l_ld : L;
+      cp_async16(&As[kk * LDS_A + i], src, ok);
+    }
+  }
+  if (t.r_op == OP_N) {
+    // R[(k0+kk) + (n0+j)*ld] : contiguous in k
+    const int kk = tid & 15;
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+      int j = (tid >> 4) + 8 * r;
+      bool ok = (n0 + j < N) && (k0 + kk < K);
+      const double2* src = ok ? R + (long long)(k0 + kk) + (long long)(n0 + j) * t.r_ld : R;
+      cp_async16(&Bs[kk * LDS_B + j], src, ok);
+    }
+  } else {
+    // op(R)[k][n] = conj(R[n + k*ld]) : contiguous in n
+    const int j = tid & 63;
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+      int kk = (tid >> 6) + 2 * r;
+      bool ok = (n0 + j < N) && (k0 + kk < K);
+      const double2* src = ok ? R + (long long)(n0 + j) + (long long)(k0 + kk) * t.r_ld : R;
+      cp_async16(&Bs[kk * LDS_B + j], src, ok);
+    }
+  }
+}
+
+__global__ void __launch_bounds__(GEMM_THREADS, 2)
+grouped_zgemm_kernel(const GJob* __restrict__ jobs, const GGroup* __restrict__ groups,
+                     const GTerm* __restrict__ terms, Bases bases) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  SmemTiles& s = *reinterpret_cast<SmemTiles*>(smem_raw);
+  const GJob job = jobs[blockIdx.x];
+  const GGroup g = groups[job.group];
+  const int m0 = job.tm * TM, n0 = job.tn * TN;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int wm = warp & 1, wn = warp >> 1;
+  const int lg = lane >> 2, lt = lane & 3;
+
+  double cre[4][4][2], cim[4][4][2];
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+      cre[a][b][0] = cre[a][b][1] = 0.0;
+      cim[a][b][0] = cim[a][b][1] = 0.0;
+    }
+
+  for (int ti = g.t0; ti < g.t1; ++ti) {
+    const GTerm t = terms[ti];
+    if (t.kind == TK_GEMM) {
+      const double2* L = bases.p[t.l_base] + t.l_off;
+      const double2* R = bases.p[t.r_base] + t.r_off;
+      const int nk = (t.K + TK - 1) / TK;
+      __syncthreads();   // previous term done with the shared tiles
+      load_tiles(s, 0, t, L, R, g.M, g.N, m0, n0, 0);
+      cp_async_commit();
+      const bool lc = t.l_op == OP_C, rc = t.r_op == OP_C;
+      for (int kt = 0; kt < nk; ++kt) {
+        if (kt + 1 < nk) {
+          load_tiles(s, (kt + 1) & 1, t, L, R, g.M, g.N, m0, n0, (kt + 1) * TK);
+          cp_async_commit();
+          cp_async_wait<1>();
+        } else {
+          cp_async_wait<0>();
+        }
+        __syncthreads();
+        const double2* As = s.a[kt & 1];
+        const double2* Bs = s.b[kt & 1];
+#pragma unroll
+        for (int kb = 0; kb < TK / 4; ++kb) {
+          const int krow = kb * 4 + lt;
+          double ar[4], ai[4], nai[4], br[4], bi[4];
+#pragma unroll
+          for (int mi = 0; mi < 4; ++mi) {
+            double2 v = As[krow * LDS_A + wm * 32 + mi * 8 + lg];
+            ar[mi] = v.x;
+            ai[mi] = lc ? -v.y : v.y;
+            nai[mi] = -ai[mi];
+          }
+#pragma unroll
+          for (int ni = 0; ni < 4; ++ni) {
+            double2 v = Bs[krow * LDS_B + wn * 32 + ni * 8 + lg];
+            double vr = v.x, vi = rc ? -v.y : v.y;
+            br[ni] = t.ar * vr - t.ai * vi;
+            bi[ni] = t.ar * vi + t.ai * vr;
+          }
+#pragma unroll
+          for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+            for (int ni = 0; ni < 4; ++ni) {
+              dmma(cre[mi][ni][0], cre[mi][ni][1], ar[mi], br[ni]);
+              dmma(cre[mi][ni][0], cre[mi][ni][1], nai[mi], bi[ni]);
+              dmma(cim[mi][ni][0], cim[mi][ni][1], ar[mi], bi[ni]);
+              dmma(cim[mi][ni][0], cim[mi][ni][1], ai[mi], br[ni]);
+            }
+        }
+        __syncthreads();
+      }
+    } else {
+      // element-wise terms on the accumulator layout
+      const double2* R = bases.p[t.r_base] + t.r_off;
+#pragma unroll
+      for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+        for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+          for (int e = 0; e < 2; ++e) {
+            int row = m0 + wm * 32 + mi * 8 + lg;
+            int col = n0 + wn * 32 + ni * 8 + 2 * lt + e;
+            int rr = row - t.r0, cc = col - t.c0;
+            if (row >= g.M || col >= g.N || rr < 0 || cc < 0 || rr >= t.rm || cc >= t.rn) continue;
+            double vr, vi;
+            if (t.kind == TK_AXPY) {
+              double2 v = (t.r_op == OP_N) ? R[(long long)rr + (long long)cc * t.r_ld]
+                                           : R[(long long)cc + (long long)rr * t.r_ld];
+              vr = v.x;
+              vi = (t.r_op == OP_C) ? -v.y : v.y;
+            } else {
+              if (rr != cc) continue;
+              vr = 1.0;
+              vi = 0.0;
+            }
+            cre[mi][ni][e] += t.ar * vr - t.ai * vi;
+            cim[mi][ni][e] += t.ar * vi + t.ai * vr;
+          }
+    }
+  }
+
+  double2* C = bases.p[g.c_base] + g.c_off;
+#pragma unroll
+  for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+    for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        int row = m0 + wm * 32 + mi * 8 + lg;
+        int col = n0 + wn * 32 + ni * 8 + 2 * lt + e;
+        if (row < g.M && col < g.N) {
+          double2* p = C + (long long)row + (long long)col * g.c_ld;
+          double2 v = make_double2(cre[mi][ni][e], cim[mi][ni][e]);
+          if (g.beta) {
+            double2 o = *p;
+            v.x += o.x;
+            v.y += o.y;
+          }
+          *p = v;
+        }
+      }
+}
+
+// ---------------------------------------------------------------- vector kernels
+constexpr int VB = 256;          // threads per block
+constexpr int VCHUNK = 8192;     // elements per block in reductions
+
+__global__ void multi_dot_partial(const double2* __restrict__ X, long long ld, int nvec,
+                                  const double2* __restrict__ y, long long n, double* __restrict__ partial,
+                                  int nblk) {
+  __shared__ double red[VB / 32];
+  long long beg = (long long)blockIdx.x * VCHUNK;
+  long long end = beg + VCHUNK < n ? beg + VCHUNK : n;
+  for (int j = 0; j < nvec; ++j) {
+    const double2* x = X + (long long)j * ld;
+    double acc = 0.0;
+    for (long long e = beg + threadIdx.x; e < end; e += VB) {
+      double2 a = x[e], b = y[e];
+      acc = fma(a.x, b.x, acc);
+      acc = fma(a.y, b.y, acc);
+    }
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double s = 0.0;
+      for (int w = 0; w < VB / 32; ++w) s += red[w];
+      partial[(long long)j * nblk + blockIdx.x] = s;
+    }
+    __syncthreads();
+  }
+}
+
+__global__ void multi_dot_final(const double* __restrict__ partial, int nblk, int nvec, double* __restrict__ out) {
+  int j = blockIdx.x;
+  if (j >= nvec) return;
+  __shared__ double red[32];
+  double acc = 0.0;
+  for (int b = threadIdx.x; b < nblk; b += blockDim.x) acc += partial[(long long)j * nblk + b];
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += red[w];
+    out[j] = s;
+  }
+}
+
+// w = w - alpha*v - beta_prev*vprev   (eigen.f90:65-75)
+__global__ void lanczos_update_kernel(double2* __restrict__ w, const double2* __restrict__ v,
+                                      const double2* __restrict__ vprev, const double* __restrict__ alpha,
+                                      const double* __restrict__ beta_prev, long long n) {
+  const double a = *alpha;
+  const double b = vprev ? *beta_prev : 0.0;
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+    double2 x = w[e], p = v[e];
+    x.x = x.x - a * p.x;
+    x.y = x.y - a * p.y;
+    if (vprev) {
+      double2 q = vprev[e];
+      x.x = x.x - b * q.x;
+      x.y = x.y - b * q.y;
+    }
+    w[e] = x;
+  }
+}
+
+// w = w / sqrt(norm2)   (wave_normalize, block.f90:1135-1150)
+__global__ void scale_kernel(double2* __restrict__ w, const double* __restrict__ norm2, long long n, int invert_sqrt) {
+  const double s = invert_sqrt ? sqrt(*norm2) : *norm2;
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+    double2 x = w[e];
+    x.x = x.x / s;
+    x.y = x.y / s;
+    w[e] = x;
+  }
+}
+
+// w = w - sum_j (uv_j/uu_j) x_j   (Gram_Schmidt_process, block.f90:1265-1285)
+__global__ void gs_subtract_kernel(double2* __restrict__ w, const double2* __restrict__ X, long long ld, int nvec,
+                                   const double* __restrict__ uv, const double* __restrict__ uu, long long n) {
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+    double tr = 0.0, tim = 0.0;
+    for (int j = 0; j < nvec; ++j) {
+      const double c = uv[j] / uu[j];
+      double2 x = X[(long long)j * ld + e];
+      tr = tr + c * x.x;
+      tim = tim + c * x.y;
+    }
+    double2 x = w[e];
+    x.x = x.x - tr;
+    x.y = x.y - tim;
+    w[e] = x;
+  }
+}
+
+// out = sum_i z_i x_i   (eigen.f90:146-153)
+__global__ void combine_kernel(double2* __restrict__ out, const double2* __restrict__ X, long long ld, int nvec,
+                               const double* __restrict__ z, long long n) {
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+    double r = 0.0, im = 0.0;
+    for (int j = 0; j < nvec; ++j) {
+      double2 x = X[(long long)j * ld + e];
+      r = r + z[j] * x.x;
+      im = im + z[j] * x.y;
+    }
+    out[e] = make_double2(r, im);
+  }
+}
+
+// number of eigenvalues of T below x (Sturm sequence)
+__device__ int sturm_count(const double* d, const double* e, int n, double x, double pivmin) {
+  int c = 0;
+  double q = d[0] - x;
+  if (fabs(q) < pivmin) q = -pivmin;
+  if (q < 0) c++;
+  for (int i = 1; i < n; ++i) {
+    q = d[i] - x - e[i - 1] * e[i - 1] / q;
+    if (fabs(q) < pivmin) q = -pivmin;
+    if (q < 0) c++;
+  }
+  return c;
+}
+
+__global__ void tridiag_lowest_kernel(const double* __restrict__ d, const double* __restrict__ e, int n,
+                                      int want_vec, double* __restrict__ res, double* __restrict__ z) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  if (n == 1) {
+    res[0] = d[0];
+    if (want_vec) z[0] = 1.0;
+    return;
+  }
+  double lo = d[0], hi = d[0], emax = 0.0;
+  for (int i = 0; i < n; ++i) {
+    double r = (i > 0 ? fabs(e[i - 1]) : 0.0) + (i < n - 1 ? fabs(e[i]) : 0.0);
+    lo = fmin(lo, d[i] - r);
+    hi = fmax(hi, d[i] + r);
+    if (i < n - 1) emax = fmax(emax, e[i] * e[i]);
+  }
+  const double tnorm = fmax(fabs(lo), fabs(hi));
+  const double pivmin = DBL_MIN * fmax(1.0, emax);
+  lo -= 2.0 * DBL_EPSILON * tnorm + pivmin;
+  hi += 2.0 * DBL_EPSILON * tnorm + pivmin;
+  // invariant: count(lo) == 0, count(hi) >= 1
+  for (int it = 0; it < 200; ++it) {
+    double mid = 0.5 * (lo + hi);
+    if (mid <= lo || mid >= hi) break;
+    if (hi - lo <= 2.0 * DBL_EPSILON * fmax(fabs(lo), fabs(hi)) + pivmin) break;
+    if (sturm_count(d, e, n, mid, pivmin) >= 1) hi = mid;
+    else lo = mid;
+  }
+  const double lam = 0.5 * (lo + hi);
+  res[0] = lam;
+  if (!want_vec) return;
+  // inverse iteration on (T - lam I) with a partially pivoted tridiagonal LU
+  // (rows kept as diag/super1/super2 of U plus multipliers); n <= 101.
+  double u0[128], u1[128], u2[128], lm[128], y[128];
+  int piv[128];
+  const double shift = lam;
+  const double tiny = DBL_EPSILON * tnorm + pivmin;
+  {
+    double a = d[0] - shift, b = (n > 1) ? e[0] : 0.0, c = 0.0;
+    for (int i = 0; i < n - 1; ++i) {
+      double sub = e[i], na = d[i + 1] - shift, nb = (i + 1 < n - 1) ? e[i + 1] : 0.0;
+      if (fabs(a) >= fabs(sub)) {
+        piv[i] = 0;
+        if (fabs(a) < tiny) a = (a < 0 ? -tiny : tiny);
+        double l = sub / a;
+        lm[i] = l;
+        u0[i] = a; u1[i] = b; u2[i] = c;
+        a = na - l * b;
+        b = nb - l * c;
+        c = 0.0;
+      } else {
+        piv[i] = 1;
+        double l = a / sub;
+        lm[i] = l;
+        u0[i] = sub; u1[i] = na; u2[i] = nb;
+        double a2 = b - l * na, b2 = c - l * nb;
+        a = a2;
+        b = b2;
+        c = 0.0;
+      }
+    }
+    if (fabs(a) < tiny) a = (a < 0 ? -tiny : tiny);
+    u0[n - 1] = a; u1[n - 1] = 0.0; u2[n - 1] = 0.0;
+  }
+  for (int i = 0; i < n; ++i) y[i] = 1.0;
+  for (int pass = 0; pass < 3; ++pass) {
+    // forward: apply row swaps and multipliers to y
+    for (int i = 0; i < n - 1; ++i) {
+      if (piv[i]) {
+        double t = y[i];
+        y[i] = y[i + 1];
+        y[i + 1] = t;
+      }
+      y[i + 1] -= lm[i] * y[i];
+    }
+    // back substitution with U (diag u0, super u1, u2)
+    for (int i = n - 1; i >= 0; --i) {
+      double s = y[i];
+      if (i + 1 < n) s -= u1[i] * y[i + 1];
+      if (i + 2 < n) s -= u2[i] * y[i + 2];
+      y[i] = s / u0[i];
+    }
+    double nrm = 0.0;
+    for (int i = 0; i < n; ++i) nrm += y[i] * y[i];
+    nrm = sqrt(nrm);
+    for (int i = 0; i < n; ++i) y[i] /= nrm;
+  }
+  int imax = 0;
+  for (int i = 1; i < n; ++i)
+    if (fabs(y[i]) > fabs(y[imax])) imax = i;
+  const double sg = y[imax] < 0 ? -1.0 : 1.0;
+  for (int i = 0; i < n; ++i) z[i] = sg * y[i];
+}
+
+__global__ void phase_fix_kernel(double2* __restrict__ U, int rows) {
+  double2* u = U + (long long)blockIdx.x * rows;
+  __shared__ double sr[32], si[32];
+  double zr = 0.0, zi = 0.0;
+  for (int r = threadIdx.x; r < rows; r += blockDim.x) {
+    double w = 1.0 / (1.0 + 0.1 * r);
+    zr += u[r].x * w;
+    zi += u[r].y * w;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    zr += __shfl_xor_sync(0xffffffffu, zr, o);
+    zi += __shfl_xor_sync(0xffffffffu, zi, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    sr[threadIdx.x >> 5] = zr;
+    si[threadIdx.x >> 5] = zi;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double a = 0.0, b = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+      a += sr[w];
+      b += si[w];
+    }
+    sr[0] = a;
+    si[0] = b;
+  }
+  __syncthreads();
+  const double a = hypot(sr[0], si[0]);
+  if (a < 1e-10) return;
+  const double fr = sr[0] / a, fi = -si[0] / a;
+  for (int r = threadIdx.x; r < rows; r += blockDim.x) {
+    double2 x = u[r];
+    u[r] = make_double2(x.x * fr - x.y * fi, x.x * fi + x.y * fr);
+  }
+}
+
+inline int grid_for(long long n) {
+  long long b = (n + VB - 1) / VB;
+  if (b > 148 * 16) b = 148 * 16;
+  if (b < 1) b = 1;
+  return (int)b;
+}
+
+}  // namespace
+
+cudaError_t launch_grouped_zgemm(const GJob* jobs, int njobs, const GGroup* groups, const GTerm* terms,
+                                 Bases bases, cudaStream_t st) {
+  if (njobs <= 0) return cudaSuccess;
+  const size_t smem = sizeof(SmemTiles);
+  static bool attr = false;
+  if (!attr) {
+    cudaError_t e = cudaFuncSetAttribute(grouped_zgemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    attr = true;
+  }
+  grouped_zgemm_kernel<<<njobs, GEMM_THREADS, smem, st>>>(jobs, groups, terms, bases);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_multi_dot(const double2* X, long long ld, int nvec, const double2* y, long long n,
+                             double* partial, double* out, cudaStream_t st) {
+  if (nvec <= 0) return cudaSuccess;
+  int nblk = (int)((n + VCHUNK - 1) / VCHUNK);
+  if (nblk < 1) nblk = 1;
+  multi_dot_partial<<<nblk, VB, 0, st>>>(X, ld, nvec, y, n, partial, nblk);
+  multi_dot_final<<<nvec, 256, 0, st>>>(partial, nblk, nvec, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_lanczos_update(double2* w, const double2* v, const double2* vprev, const double* alpha,
+                                  const double* beta_prev, long long n, cudaStream_t st) {
+  lanczos_update_kernel<<<grid_for(n), VB, 0, st>>>(w, v, vprev, alpha, beta_prev, n);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_scale(double2* w, const double* norm2, long long n, int invert_sqrt, cudaStream_t st) {
+  scale_kernel<<<grid_for(n), VB, 0, st>>>(w, norm2, n, invert_sqrt);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_gs_subtract(double2* w, const double2* X, long long ld, int nvec, const double* uv,
+                               const double* uu, long long n, cudaStream_t st) {
+  gs_subtract_kernel<<<grid_for(n), VB, 0, st>>>(w, X, ld, nvec, uv, uu, n);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_combine(double2* out, const double2* X, long long ld, int nvec, const double* z, long long n,
+                           cudaStream_t st) {
+  combine_kernel<<<grid_for(n), VB, 0, st>>>(out, X, ld, nvec, z, n);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_phase_fix(double2* U, int rows, int cols, cudaStream_t st) {
+  if (rows <= 0 || cols <= 0) return cudaSuccess;
+  phase_fix_kernel<<<cols, 128, 0, st>>>(U, rows);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_tridiag_lowest(const double* d, const double* e, int n, int want_vec, double* res, double* z,
+                                  cudaStream_t st) {
+  if (n > 128) return cudaErrorInvalidValue;
+  tridiag_lowest_kernel<<<1, 32, 0, st>>>(d, e, n, want_vec, res, z);
+  return cudaGetLastError();
+}
+
+}  // namespace tsc

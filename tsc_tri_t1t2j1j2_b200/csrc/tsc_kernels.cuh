@@ -1,0 +1,73 @@
+// Device task formats shared by the host task builders and the kernels.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+
+namespace tsc {
+
+// Operand pointer = base[id] + off (complex128 elements).  Base 0 is the null
+// pointer (off is then an absolute address / 16); bases 1..3 are rebound per
+// launch (input vector, output vector, scratch) so one task list serves every
+// Lanczos iteration.
+enum BaseId : uint8_t { BASE_ABS = 0, BASE_IN = 1, BASE_OUT = 2, BASE_SCR = 3 };
+enum TermKind : uint8_t { TK_GEMM = 0, TK_AXPY = 1, TK_DIAG = 2 };
+enum Op : uint8_t { OP_N = 0, OP_C = 1 };
+
+// One contribution to an output group:
+//   GEMM:  C += alpha * op(L)[M x K] * op(R)[K x N]          (whole group)
+//   AXPY:  C[r0:r0+rm, c0:c0+rn] += alpha * op(R)[rm x rn]
+//   DIAG:  C[r0+i, c0+i] += alpha   for i < rm
+struct GTerm {
+  long long l_off, r_off;
+  int l_ld, r_ld;
+  int K;
+  int r0, c0, rm, rn;
+  double ar, ai;
+  uint8_t l_base, r_base, l_op, r_op, kind, pad0, pad1, pad2;
+};
+
+// Output rectangle C (M x N, column-major, leading dimension c_ld).  After the
+// launch C = sum(terms) + beta * C_old; every element of C is written.
+struct GGroup {
+  long long c_off;
+  int c_ld, M, N;
+  int t0, t1;
+  uint8_t c_base, beta, pad0, pad1;
+};
+
+struct GJob {
+  int group, tm, tn, pad;
+};
+
+struct Bases {
+  double2* p[4];
+};
+
+constexpr int GEMM_TM = 64, GEMM_TN = 64, GEMM_TK = 16, GEMM_THREADS = 128;
+
+cudaError_t launch_grouped_zgemm(const GJob* jobs, int njobs, const GGroup* groups, const GTerm* terms,
+                                 Bases bases, cudaStream_t st);
+
+// ---- vector kernels (Lanczos, eigen.f90 / block.f90:1092-1354) -------------------
+// partial sums of Re<x_j, y> for j < nvec (x_j = X + j*ld), deterministic two-pass
+cudaError_t launch_multi_dot(const double2* X, long long ld, int nvec, const double2* y, long long n,
+                             double* partial, double* out, cudaStream_t st);
+cudaError_t launch_lanczos_update(double2* w, const double2* v, const double2* vprev, const double* alpha,
+                                  const double* beta_prev, long long n, cudaStream_t st);
+cudaError_t launch_scale(double2* w, const double* norm2, long long n, int invert_sqrt, cudaStream_t st);
+cudaError_t launch_gs_subtract(double2* w, const double2* X, long long ld, int nvec, const double* uv,
+                               const double* uu, long long n, cudaStream_t st);
+cudaError_t launch_combine(double2* out, const double2* X, long long ld, int nvec, const double* z,
+                           long long n, cudaStream_t st);
+
+// Canonical phase of each column of U (rows x cols, column-major): u *= conj(z)/|z|
+// with z = sum_r u_r / (1 + r/10).  Eigensolvers return arbitrary phases; fixing
+// them makes renormalised operators independent of the eigensolver.
+cudaError_t launch_phase_fix(double2* U, int rows, int cols, cudaStream_t st);
+
+// tridiagonal lowest eigenpair (dstev stand-in): d[0..n), e[0..n-1); writes
+// res[0]=E0 and, if want_vec, z[0..n) the normalised eigenvector.
+cudaError_t launch_tridiag_lowest(const double* d, const double* e, int n, int want_vec, double* res,
+                                  double* z, cudaStream_t st);
+
+}  // namespace tsc

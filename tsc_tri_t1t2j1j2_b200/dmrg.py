@@ -1,0 +1,186 @@
+"""Python mirror of the reference's hot-path interface over the C-ABI.
+
+Method names follow the Fortran subroutines they replace:
+
+=========================  ==============================================
+method                     reference
+=========================  ==============================================
+``model_wave``             get_sys.f90:6915 (H.psi, after hmerge :7398)
+``lanczos_memo_new``       eigen.f90:4
+``get_truncation_operator`` den_mat.f90:106/146 + :184
+``get_hamiltonian``        get_sys.f90:4 (sys) / :305 (env)
+``wave_trans``             dmrg_sub.f90:1471 (LR) / :1637 (RL)
+``get_ground_state``       main.f90:114 (warm-up + sweeps)
+=========================  ==============================================
+
+Arguments are the flat descriptor objects of ``layout``; every call runs on
+the GPU (there is no CPU path) and raises ``TscError`` with the library's
+status code and message on failure.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from .layout import Basis, Block, Cursor, Model, Wave, pack
+
+P = ctypes.POINTER
+
+
+def _dptr(a):
+    return a.ctypes.data_as(P(ctypes.c_double))
+
+
+def _iptr(a):
+    return a.ctypes.data_as(P(ctypes.c_int))
+
+
+class Context:
+    """One device-resident model (lattice + couplings) and its current superblock."""
+
+    def __init__(self, Nx, Ny, t1=1.0, t2=0.0, J1=0.4, J2=0.0, delta=12, device=0):
+        self.L = _lib.load()
+        cfg = _lib.ModelConfig(Nx, Ny, t1, t2, J1, J2, delta, device)
+        h = ctypes.c_void_p()
+        rc = self.L.tsc_create(ctypes.byref(h), ctypes.byref(cfg))
+        self.h = h
+        if rc != 0:
+            msg = self.L.tsc_last_error(h).decode() if h else "tsc_create failed"
+            if h:
+                self.L.tsc_destroy(h)
+            self.h = None
+            raise _lib.TscError(rc, msg)
+        self.Nx, self.Ny = Nx, Ny
+        self.sys_len = self.env_len = 0
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.tsc_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def _check(self, rc):
+        if rc < 0:
+            raise _lib.TscError(rc, self.L.tsc_last_error(self.h).decode())
+        return rc
+
+    @property
+    def tot_num_up(self):
+        return self.L.tsc_tot_num_up(self.h)
+
+    # ---------------------------------------------------------------- superblock
+    def set_superblock(self, sys: Model, env: Model, sys_bs: Basis, env_bs: Basis, layout: Wave):
+        ints, data = [], []
+        sys.write(ints, data)
+        env.write(ints, data)
+        sys_bs.write(ints, data)
+        env_bs.write(ints, data)
+        layout.write(ints, data, with_data=False)
+        self.set_superblock_flat(sys.len, env.len, *pack(ints, data))
+        self.layout = layout
+
+    def set_superblock_flat(self, sys_len, env_len, ints, data):
+        ints = np.ascontiguousarray(ints, np.int32)
+        data = np.ascontiguousarray(data, np.complex128)
+        self._check(self.L.tsc_superblock_set(self.h, sys_len, env_len, _iptr(ints), len(ints), _dptr(data), len(data)))
+        self.sys_len, self.env_len = sys_len, env_len
+        self.dim = self.L.tsc_superblock_dim(self.h)
+
+    def model_wave(self, vec):
+        """out = H vec (host buffers, copies included)."""
+        x = np.ascontiguousarray(vec, np.complex128)
+        if len(x) != self.dim:
+            raise ValueError("vector length does not match the superblock")
+        out = np.empty_like(x)
+        self._check(self.L.tsc_hpsi(self.h, _dptr(x), _dptr(out)))
+        return out
+
+    def hpsi_device(self, d_in: int, d_out: int):
+        """H.psi on device pointers (e.g. torch tensors' data_ptr()), enqueued on the context stream."""
+        self._check(self.L.tsc_hpsi_device(self.h, ctypes.c_void_p(d_in), ctypes.c_void_p(d_out)))
+
+    def hpsi_stats(self):
+        ms, rf, ef, nl = ctypes.c_double(), ctypes.c_double(), ctypes.c_double(), ctypes.c_int()
+        self._check(self.L.tsc_hpsi_stats(self.h, ctypes.byref(ms), ctypes.byref(rf), ctypes.byref(ef), ctypes.byref(nl)))
+        return {"device_ms": ms.value, "ref_flops": rf.value, "exec_flops": ef.value, "launches": nl.value}
+
+    def lanczos_memo_new(self, vec, lanzero):
+        x = np.ascontiguousarray(vec, np.complex128).copy()
+        it, e0 = ctypes.c_int(), ctypes.c_double()
+        self._check(self.L.tsc_lanczos(self.h, _dptr(x), lanzero, ctypes.byref(it), ctypes.byref(e0)))
+        return x, e0.value, it.value
+
+    def get_truncation_operator(self, side, vec, kept_min, kept_max, trun_err):
+        """side 0: sys density matrix (den_mat.f90:106), 1: env (den_mat.f90:146)."""
+        x = np.ascontiguousarray(vec, np.complex128)
+        ns = ctypes.c_int()
+        err, ent, entm = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        ti, tn, td, tc = P(ctypes.c_int)(), ctypes.c_longlong(), P(ctypes.c_double)(), ctypes.c_longlong()
+        spec = np.zeros(max(1, int(self.dim)), np.float64)
+        self._check(self.L.tsc_truncate(self.h, side, _dptr(x), kept_min, kept_max, trun_err, ctypes.byref(ns),
+                                        ctypes.byref(err), ctypes.byref(ent), ctypes.byref(entm), ctypes.byref(ti),
+                                        ctypes.byref(tn), ctypes.byref(td), ctypes.byref(tc), _dptr(spec), len(spec)))
+        ints = np.ctypeslib.as_array(ti, shape=(tn.value,)).copy()
+        data = (np.ctypeslib.as_array(td, shape=(2 * tc.value,)).copy().view(np.complex128)
+                if tc.value else np.zeros(0, np.complex128))
+        trun = Block.read(Cursor(ints, data))
+        return {"trun": trun, "num_state": ns.value, "err": err.value, "entropy": ent.value,
+                "entropy_mult": entm.value, "spectrum": spec}
+
+    def get_hamiltonian(self, side, model: Model, basis: Basis, trun: Block, sys_len, env_len, mshift=0):
+        """Get_Hamiltonian_Sys (side 0) / Get_Hamiltonian_Env (side 1): enlarge + renormalise."""
+        ints, data = [], []
+        model.write(ints, data)
+        basis.write(ints, data)
+        trun.write(ints, data)
+        ints, data = pack(ints, data)
+        oi, on, od, oc = P(ctypes.c_int)(), ctypes.c_longlong(), P(ctypes.c_double)(), ctypes.c_longlong()
+        self._check(self.L.tsc_renormalize(self.h, side, sys_len, env_len, mshift, _iptr(ints), len(ints), _dptr(data),
+                                           len(data), ctypes.byref(oi), ctypes.byref(on), ctypes.byref(od),
+                                           ctypes.byref(oc)))
+        gi = np.ctypeslib.as_array(oi, shape=(on.value,)).copy()
+        gd = (np.ctypeslib.as_array(od, shape=(2 * oc.value,)).copy().view(np.complex128)
+              if oc.value else np.zeros(0, np.complex128))
+        return Model.read(Cursor(gi, gd))
+
+    def wave_trans(self, direction, sys_bs: Basis, env_bs: Basis, sys_trun: Block, env_trun: Block, old: Wave,
+                   new_layout: Wave) -> Wave:
+        """direction 0: wave_trans_LR, 1: wave_trans_RL."""
+        ints, data = [], []
+        sys_bs.write(ints, data)
+        env_bs.write(ints, data)
+        sys_trun.write(ints, data)
+        env_trun.write(ints, data)
+        old.write(ints, data)
+        new_layout.write(ints, data, with_data=False)
+        ints, data = pack(ints, data)
+        out = np.zeros(new_layout.dim, np.complex128)
+        self._check(self.L.tsc_wave_transform(self.h, direction, _iptr(ints), len(ints), _dptr(data), len(data),
+                                              _dptr(out)))
+        return Wave(new_layout.sys_len, new_layout.env_len, new_layout.secs, out)
+
+    # ------------------------------------------------------------------ full run
+    def get_ground_state(self, kept_min, kept_warm, sweeps, lanzero=-1.0, seed=1, capture_step=-1, max_steps=100000):
+        self._check(self.L.tsc_set_capture(self.h, capture_step))
+        sk = (ctypes.c_int * max(1, len(sweeps)))(*sweeps)
+        cfg = _lib.SweepConfig(kept_min, kept_warm, len(sweeps), sk, lanzero, seed)
+        logs = (_lib.StepLog * max_steps)()
+        n = self._check(self.L.tsc_dmrg_run(self.h, ctypes.byref(cfg), logs, max_steps))
+        out = []
+        for k in range(min(n, max_steps)):
+            s = logs[k]
+            out.append({f: getattr(s, f) for f, _ in _lib.StepLog._fields_})
+        return out
+
+    def capture(self):
+        ti, tn, td, tc = P(ctypes.c_int)(), ctypes.c_longlong(), P(ctypes.c_double)(), ctypes.c_longlong()
+        sl, el = ctypes.c_int(), ctypes.c_int()
+        self._check(self.L.tsc_get_capture(self.h, ctypes.byref(ti), ctypes.byref(tn), ctypes.byref(td),
+                                           ctypes.byref(tc), ctypes.byref(sl), ctypes.byref(el)))
+        ints = np.ctypeslib.as_array(ti, shape=(tn.value,)).copy()
+        data = np.ctypeslib.as_array(td, shape=(2 * tc.value,)).copy().view(np.complex128)
+        return ints, data, sl.value, el.value
