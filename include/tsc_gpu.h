@@ -53,6 +53,7 @@ typedef struct tsc_sweep_config {
   const int* sweep_kept_max;   /* nsweeps entries */
   double lanzero;          /* >0: Lanczos tolerance in every phase; <=0: reference schedule */
   unsigned long long seed; /* random initial states (block.f90:1154-1180 stand-in) */
+  int warmup_only;         /* 1: stop after warm_up_point (dmrg_sub.f90:974-1147) */
 } tsc_sweep_config;
 
 /* One record per Lanczos solve (eigen.f90:169-173, den_mat.f90:342-350). */
@@ -144,6 +145,10 @@ int tsc_get_capture(tsc_ctx* ctx, const int** ints, long long* nints, const doub
  * flops of one model_wave in the reference's GEMM association order, the flops
  * the kernels execute (fewer: shared left products), and the launch count. */
 int tsc_hpsi_stats(tsc_ctx* ctx, double* device_ms, double* ref_flops, double* exec_flops, int* launches);
+
+/* The context's CUDA stream (cudaStream_t as void*): device-pointer calls are
+ * enqueued on it, so callers can order their own work and time it with events. */
+void* tsc_stream(tsc_ctx* ctx);
 
 #ifdef __cplusplus
 }

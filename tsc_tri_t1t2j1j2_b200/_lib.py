@@ -19,7 +19,7 @@ EXPORTED = [
     "tsc_create", "tsc_destroy", "tsc_last_error", "tsc_tot_num_up", "tsc_superblock_set",
     "tsc_superblock_dim", "tsc_hpsi", "tsc_hpsi_device", "tsc_lanczos", "tsc_truncate",
     "tsc_renormalize", "tsc_wave_transform", "tsc_dmrg_run", "tsc_set_capture", "tsc_get_capture",
-    "tsc_hpsi_stats",
+    "tsc_hpsi_stats", "tsc_stream",
 ]
 
 
@@ -30,7 +30,8 @@ class ModelConfig(ctypes.Structure):
 
 class SweepConfig(ctypes.Structure):
     _fields_ = [("kept_min", c_int), ("kept_max_warmup", c_int), ("nsweeps", c_int),
-                ("sweep_kept_max", P(c_int)), ("lanzero", c_double), ("seed", ctypes.c_ulonglong)]
+                ("sweep_kept_max", P(c_int)), ("lanzero", c_double), ("seed", ctypes.c_ulonglong),
+                ("warmup_only", c_int)]
 
 
 class StepLog(ctypes.Structure):
@@ -78,6 +79,8 @@ def load():
     L.tsc_set_capture.argtypes = [c_void, c_int]
     L.tsc_get_capture.argtypes = [c_void, P(pi), P(c_ll), P(pd), P(c_ll), pi, pi]
     L.tsc_hpsi_stats.argtypes = [c_void, pd, pd, pd, pi]
+    L.tsc_stream.argtypes = [c_void]
+    L.tsc_stream.restype = c_void
     _lib = L
     return L
 

@@ -351,7 +351,7 @@ int tsc_dmrg_run(tsc_ctx* ctx, const tsc_sweep_config* sw, tsc_step_log* log, in
     if (sw->kept_min < 1 || sw->kept_max_warmup < 1) throw Error(TSC_E_ARG, "kept sizes must be positive");
     std::vector<int> sweeps(sw->sweep_kept_max, sw->sweep_kept_max + sw->nsweeps);
     std::vector<Engine::StepRec> recs;
-    ctx->eng->run(sw->kept_min, sw->kept_max_warmup, sweeps, sw->lanzero, sw->seed, &recs);
+    ctx->eng->run(sw->kept_min, sw->kept_max_warmup, sweeps, sw->lanzero, sw->seed, &recs, sw->warmup_only != 0);
     nsteps = (int)recs.size();
     for (int i = 0; i < nsteps && i < max_steps && log; ++i) {
       const auto& s = recs[i];
@@ -361,6 +361,8 @@ int tsc_dmrg_run(tsc_ctx* ctx, const tsc_sweep_config* sw, tsc_step_log* log, in
   });
   return rc == TSC_OK ? nsteps : rc;
 }
+
+void* tsc_stream(tsc_ctx* ctx) { return (ctx && ctx->eng) ? (void*)ctx->eng->st : nullptr; }
 
 int tsc_set_capture(tsc_ctx* ctx, int capture_step) {
   return guard(ctx, [&] {

@@ -1298,7 +1298,7 @@ void Engine::right_to_left(int bg_id, int end_id, double trun_err, std::vector<S
 }
 
 void Engine::run(int kept_min, int kept_warm, const std::vector<int>& sweeps, double lanzero_override,
-                 unsigned long long seed, std::vector<StepRec>* log) {
+                 unsigned long long seed, std::vector<StepRec>* log, bool warmup_only) {
   const int N = L.num_site;
   rng = seed;
   nsolve_ = 0;
@@ -1315,6 +1315,7 @@ void Engine::run(int kept_min, int kept_warm, const std::vector<int>& sweeps, do
   restart1 = 0;
   lanzero_ = lz(lanerr * 1000);
   warm_up(N / 2, trun_err * 100, log);
+  if (warmup_only) return;
   lanzero_ = lz(lanerr * 15);
   double tmp_err = trun_err * 15;
   left_to_right(N / 2 - 1, N - 2, tmp_err, log);

@@ -222,7 +222,7 @@ class Engine {
     double hpsi_seconds, hpsi_flops, step_seconds;
   };
   void run(int kept_min, int kept_warm, const std::vector<int>& sweeps, double lanzero_override,
-           unsigned long long seed, std::vector<StepRec>* log);
+           unsigned long long seed, std::vector<StepRec>* log, bool warmup_only = false);
   int capture_step = -1;
   struct Capture {
     bool valid = false;

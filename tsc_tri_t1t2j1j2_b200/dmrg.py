@@ -103,6 +103,11 @@ class Context:
         """H.psi on device pointers (e.g. torch tensors' data_ptr()), enqueued on the context stream."""
         self._check(self.L.tsc_hpsi_device(self.h, ctypes.c_void_p(d_in), ctypes.c_void_p(d_out)))
 
+    @property
+    def stream(self) -> int:
+        """cudaStream_t of this context (device-pointer calls are enqueued on it)."""
+        return self.L.tsc_stream(self.h) or 0
+
     def hpsi_stats(self):
         ms, rf, ef, nl = ctypes.c_double(), ctypes.c_double(), ctypes.c_double(), ctypes.c_int()
         self._check(self.L.tsc_hpsi_stats(self.h, ctypes.byref(ms), ctypes.byref(rf), ctypes.byref(ef), ctypes.byref(nl)))
@@ -164,10 +169,11 @@ class Context:
         return Wave(new_layout.sys_len, new_layout.env_len, new_layout.secs, out)
 
     # ------------------------------------------------------------------ full run
-    def get_ground_state(self, kept_min, kept_warm, sweeps, lanzero=-1.0, seed=1, capture_step=-1, max_steps=100000):
+    def get_ground_state(self, kept_min, kept_warm, sweeps, lanzero=-1.0, seed=1, capture_step=-1, max_steps=100000,
+                         warmup_only=False):
         self._check(self.L.tsc_set_capture(self.h, capture_step))
         sk = (ctypes.c_int * max(1, len(sweeps)))(*sweeps)
-        cfg = _lib.SweepConfig(kept_min, kept_warm, len(sweeps), sk, lanzero, seed)
+        cfg = _lib.SweepConfig(kept_min, kept_warm, len(sweeps), sk, lanzero, seed, 1 if warmup_only else 0)
         logs = (_lib.StepLog * max_steps)()
         n = self._check(self.L.tsc_dmrg_run(self.h, ctypes.byref(cfg), logs, max_steps))
         out = []
