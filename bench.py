@@ -147,6 +147,14 @@ def dist_setup():
     return dist, rank, ws, local
 
 
+def max_over_ranks(x, dist, device):
+    """Max of a per-rank float over the process group (timings are max over ranks)."""
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def fp64_peak_tflops(torch, dev):
     """cuBLAS ZGEMM throughput (8 n^3 flops), best of 5: the FP64 denominator."""
     n = 4096
@@ -246,9 +254,7 @@ def run_gpu(args):
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1)
     if dist is not None:
-        t = torch.tensor([ms], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+        ms = max_over_ranks(ms, dist, dev)
         dist.barrier()
     value = ws * args.steps * ref_flops / (ms * 1e-3) / 1e12
     # per-launch kernel time of the grouped GEMM (both H.psi launches), CUDA events on the engine stream
@@ -274,9 +280,7 @@ def run_gpu(args):
         L.tsc_hpsi(ctx.h, xp, yp)
     e2e_s = time.perf_counter() - t0
     if dist is not None:
-        t = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
+        e2e_s = max_over_ranks(e2e_s, dist, dev)
     e2e = ws * ke2e * ref_flops / e2e_s / 1e12
     line = None
     if rank == 0:
