@@ -143,11 +143,18 @@ struct TaskList {
   GJob* d_jobs = nullptr;
   GGroup* d_groups = nullptr;
   GTerm* d_terms = nullptr;
-  int njobs = 0;
+  GReduce* d_reds = nullptr;
+  int njobs = 0, nreds = 0;
+  int tile = 64;           // CTA tile edge used for this list (64 or 32)
+  long long max_red_elems = 0;
+  DevBufP part;            // partial tiles of split groups
   double exec_flops = 0;   // flops the kernel executes
   long long nterms = 0;
   int add_group(double2* abs_c, uint8_t base, long long c_off, int ld, int M, int N, int beta);
-  void upload(cudaStream_t st);
+  // Packs the lists for the device.  Groups whose term list is much longer than
+  // total_cost / (slots * waves) are split into contiguous term chunks, each
+  // computing a partial tile; a fixed-order reduction then writes the group.
+  void upload(cudaStream_t st, int slots = 296, int waves = 4);
 };
 
 struct Stats {

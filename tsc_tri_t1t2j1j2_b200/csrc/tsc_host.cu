@@ -2,6 +2,7 @@
 // site operators, bases and task-list packing.
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 
 #include "tsc_engine.hpp"
@@ -346,52 +347,110 @@ int TaskList::add_group(double2* abs_c, uint8_t base, long long c_off, int ld, i
   return (int)groups.size() - 1;
 }
 
-void TaskList::upload(cudaStream_t st) {
+// CTA tile edge of the grouped GEMM: 32x32 (6 CTAs/SM) by default; TSC_TILE=64
+// selects 64x64 tiles (2 CTAs/SM), kept for comparison.
+int default_tile() {
+  static int t = [] {
+    const char* e = std::getenv("TSC_TILE");
+    return (e && std::atoi(e) == 64) ? 64 : 32;
+  }();
+  return t;
+}
+
+void TaskList::upload(cudaStream_t st, int slots, int waves) {
+  tile = default_tile();
+  const int TMt = tile, TNt = tile;
+  if (tile == 32) slots *= 3;
   std::vector<GTerm> terms;
-  std::vector<GJob> jobs;
   struct JC {
     GJob j;
     long long cost;
   };
   std::vector<JC> jc;
+  std::vector<GReduce> reds;
   exec_flops = 0;
+  auto tcost = [](const GTerm& t) -> long long {
+    return t.kind == TK_GEMM ? (long long)(t.K + GEMM_TK - 1) / GEMM_TK + 1 : 1;
+  };
+  // pass 1: flatten terms and total cost
+  std::vector<long long> gcost(groups.size(), 0);
+  long long total = 0;
   for (size_t gi = 0; gi < groups.size(); ++gi) {
     GGroup& g = groups[gi];
     g.t0 = (int)terms.size();
-    long long cost = 1;
+    long long c = 1;
     for (auto& t : gterms[gi]) {
       terms.push_back(t);
-      if (t.kind == TK_GEMM) {
-        cost += (t.K + GEMM_TK - 1) / GEMM_TK * 4;
-        exec_flops += 8.0 * g.M * g.N * t.K;
-      } else {
-        cost += 1;
-      }
+      c += tcost(t);
+      if (t.kind == TK_GEMM) exec_flops += 8.0 * g.M * g.N * t.K;
     }
     g.t1 = (int)terms.size();
+    gcost[gi] = c;
+    if (g.M > 0 && g.N > 0)
+      total += c * (long long)((g.M + TMt - 1) / TMt) * ((g.N + TNt - 1) / TNt);
+  }
+  const long long target = std::max<long long>(8, total / std::max(1, slots * waves));
+  long long part_elems = 0;
+  // pass 2: jobs, splitting long groups into term chunks of about `target`
+  for (size_t gi = 0; gi < groups.size(); ++gi) {
+    const GGroup& g = groups[gi];
     if (g.M <= 0 || g.N <= 0) continue;
-    int tm = (g.M + GEMM_TM - 1) / GEMM_TM, tn = (g.N + GEMM_TN - 1) / GEMM_TN;
-    for (int a = 0; a < tm; ++a)
-      for (int b = 0; b < tn; ++b) jc.push_back({GJob{(int)gi, a, b, 0}, cost});
+    int tm = (g.M + TMt - 1) / TMt, tn = (g.N + TNt - 1) / TNt;
+    int nchunk = (int)std::min<long long>((gcost[gi] + target - 1) / target, std::max(1, g.t1 - g.t0));
+    if (gcost[gi] <= target + target / 2 || nchunk <= 1) {
+      for (int a = 0; a < tm; ++a)
+        for (int b = 0; b < tn; ++b) jc.push_back({GJob{(int)gi, a, b, g.t0, g.t1, -1, 0}, gcost[gi]});
+      continue;
+    }
+    // contiguous chunks of roughly equal cost
+    std::vector<int> cut{g.t0};
+    long long acc = 0, per = (gcost[gi] + nchunk - 1) / nchunk;
+    for (int t = g.t0; t < g.t1; ++t) {
+      acc += tcost(terms[t]);
+      if (acc >= per && t + 1 < g.t1 && (int)cut.size() < nchunk) {
+        cut.push_back(t + 1);
+        acc = 0;
+      }
+    }
+    cut.push_back(g.t1);
+    int P = (int)cut.size() - 1;
+    long long base = part_elems;
+    long long mn = (long long)g.M * g.N;
+    part_elems += P * mn;
+    for (int p = 0; p < P; ++p) {
+      long long c = 1;
+      for (int t = cut[p]; t < cut[p + 1]; ++t) c += tcost(terms[t]);
+      for (int a = 0; a < tm; ++a)
+        for (int b = 0; b < tn; ++b) jc.push_back({GJob{(int)gi, a, b, cut[p], cut[p + 1], p, base + p * mn}, c});
+    }
+    reds.push_back(GReduce{(int)gi, P, base});
+    max_red_elems = std::max(max_red_elems, mn);
   }
   // longest jobs first: the hardware scheduler then approximates LPT balancing
   std::stable_sort(jc.begin(), jc.end(), [](const JC& a, const JC& b) { return a.cost > b.cost; });
+  std::vector<GJob> jobs;
+  jobs.reserve(jc.size());
   for (auto& x : jc) jobs.push_back(x.j);
   njobs = (int)jobs.size();
+  nreds = (int)reds.size();
   nterms = (long long)terms.size();
-  size_t bj = jobs.size() * sizeof(GJob), bg = groups.size() * sizeof(GGroup), bt = terms.size() * sizeof(GTerm);
+  size_t bj = jobs.size() * sizeof(GJob), bg = groups.size() * sizeof(GGroup), bt = terms.size() * sizeof(GTerm),
+         br = reds.size() * sizeof(GReduce);
   auto al = [](size_t x) { return (x + 255) / 256 * 256; };
-  size_t total = al(bj) + al(bg) + al(bt) + 256;
-  dev = std::make_shared<DevBuf>((total + 15) / 16, st, false);
+  size_t total_b = al(bj) + al(bg) + al(bt) + al(br) + 256;
+  dev = std::make_shared<DevBuf>((total_b + 15) / 16, st, false);
   char* base = reinterpret_cast<char*>(dev->p);
   d_jobs = reinterpret_cast<GJob*>(base);
   d_groups = reinterpret_cast<GGroup*>(base + al(bj));
   d_terms = reinterpret_cast<GTerm*>(base + al(bj) + al(bg));
-  std::vector<char> host(total, 0);
+  d_reds = reinterpret_cast<GReduce*>(base + al(bj) + al(bg) + al(bt));
+  std::vector<char> host(total_b, 0);
   if (bj) std::memcpy(host.data(), jobs.data(), bj);
   if (bg) std::memcpy(host.data() + al(bj), groups.data(), bg);
   if (bt) std::memcpy(host.data() + al(bj) + al(bg), terms.data(), bt);
-  cuda_check(cudaMemcpyAsync(base, host.data(), total, cudaMemcpyHostToDevice, st), "task upload");
+  if (br) std::memcpy(host.data() + al(bj) + al(bg) + al(bt), reds.data(), br);
+  cuda_check(cudaMemcpyAsync(base, host.data(), total_b, cudaMemcpyHostToDevice, st), "task upload");
+  part = part_elems ? std::make_shared<DevBuf>((size_t)part_elems, st, false) : nullptr;
   cuda_check(cudaStreamSynchronize(st), "task upload sync");
   gterms.clear();
   gterms.shrink_to_fit();
@@ -403,7 +462,10 @@ void Engine::run_tasks(TaskList& tl, double2* in, double2* out, double2* scr) {
   b.p[1] = in;
   b.p[2] = out;
   b.p[3] = scr;
-  cuda_check(launch_grouped_zgemm(tl.d_jobs, tl.njobs, tl.d_groups, tl.d_terms, b, st), "grouped_zgemm");
+  b.part = tl.part ? tl.part->p : nullptr;
+  cuda_check(launch_grouped_zgemm(tl.d_jobs, tl.njobs, tl.d_groups, tl.d_terms, b, st, tl.tile), "grouped_zgemm");
+  if (tl.nreds)
+    cuda_check(launch_reduce_partials(tl.d_reds, tl.nreds, tl.d_groups, b, tl.max_red_elems, st), "reduce_partials");
 }
 
 // ---- block transfer ----------------------------------------------------------------------

@@ -997,7 +997,7 @@ void Engine::hpsi(const double2* d_in, double2* d_out) {
   run_tasks(sb.p1, const_cast<double2*>(d_in), d_out, sb.scratch->p);
   run_tasks(sb.p2, const_cast<double2*>(d_in), d_out, sb.scratch->p);
   cuda_check(cudaEventRecord(ev1, st), "event");
-  last_stats.launches = (sb.p1.njobs > 0) + (sb.p2.njobs > 0);
+  last_stats.launches = (sb.p1.njobs > 0) + (sb.p2.njobs > 0) + (sb.p1.nreds > 0) + (sb.p2.nreds > 0);
   last_stats.hpsi_flops = sb.ref_flops;
 }
 

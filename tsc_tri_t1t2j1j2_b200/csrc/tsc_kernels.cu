@@ -34,93 +34,105 @@ __device__ __forceinline__ void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
 }
 __device__ __forceinline__ void dmma(double& c0, double& c1, double a, double b) {
-  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+  asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
                : "+d"(c0), "+d"(c1)
                : "d"(a), "d"(b));
 }
 
-constexpr int TM = GEMM_TM, TN = GEMM_TN, TK = GEMM_TK;
-constexpr int LDS_A = TM + 2, LDS_B = TN + 2;   // complex elements per shared row
-constexpr int STAGE_A = TK * LDS_A, STAGE_B = TK * LDS_B;
+constexpr int TK = GEMM_TK;
 
+template <int TM, int TN>
 struct SmemTiles {
-  double2 a[2][STAGE_A];
-  double2 b[2][STAGE_B];
+  static constexpr int LDS_A = TM + 2, LDS_B = TN + 2;   // complex per shared row (+2: no bank conflicts)
+  double2 a[2][TK * LDS_A];
+  double2 b[2][TK * LDS_B];
 };
 
-// Stage op(L)[m0.., k0..] (TM x TK) and op(R)[k0.., n0..] (TK x TN) into shared memory.
-__device__ __forceinline__ void load_tiles(SmemTiles& s, int stage, const GTerm& t, const double2* L,
+// Stage op(L)[m0.., k0..] (TM x TK) and op(R)[k0.., n0..] (TK x TN) into shared memory
+// with 128 threads; every 16-byte copy is a single complex element.
+template <int TM, int TN>
+__device__ __forceinline__ void load_tiles(SmemTiles<TM, TN>& s, int stage, const GTerm& t, const double2* L,
                                            const double2* R, int M, int N, int m0, int n0, int k0) {
+  constexpr int LDA = SmemTiles<TM, TN>::LDS_A, LDB = SmemTiles<TM, TN>::LDS_B;
   const int tid = threadIdx.x;
   const int K = t.K;
   double2* As = s.a[stage];
   double2* Bs = s.b[stage];
   if (t.l_op == OP_N) {
     // L[(m0+i) + (k0+kk)*ld] : contiguous in i
-    const int i = tid & 63;
+    const int i = tid % TM;
 #pragma unroll
-    for (int r = 0; r < 8; ++r) {
-      int kk = (tid >> 6) + 2 * r;
+    for (int r = 0; r < TM * TK / GEMM_THREADS; ++r) {
+      int kk = tid / TM + (GEMM_THREADS / TM) * r;
       bool ok = (m0 + i < M) && (k0 + kk < K);
       const double2* src = ok ? L + (long long)(m0 + i) + (long long)(k0 + kk) * t.l_ld : L;
-      cp_async16(&As[kk * LDS_A + i], src, ok);
+      cp_async16(&As[kk * LDA + i], src, ok);
     }
   } else {
     // op(L)[m][k] = conj(L[k + m*ld]) : contiguous in k
     const int kk = tid & 15;
 #pragma unroll
-    for (int r = 0; r < 8; ++r) {
+    for (int r = 0; r < TM * TK / GEMM_THREADS; ++r) {
       int i = (tid >> 4) + 8 * r;
       bool ok = (m0 + i < M) && (k0 + kk < K);
       const double2* src = ok ? L + (long long)(k0 + kk) + (long long)(m0 + i) * t.l_ld : L;
-      cp_async16(&As[kk * LDS_A + i], src, ok);
+      cp_async16(&As[kk * LDA + i], src, ok);
     }
   }
   if (t.r_op == OP_N) {
     // R[(k0+kk) + (n0+j)*ld] : contiguous in k
     const int kk = tid & 15;
 #pragma unroll
-    for (int r = 0; r < 8; ++r) {
+    for (int r = 0; r < TN * TK / GEMM_THREADS; ++r) {
       int j = (tid >> 4) + 8 * r;
       bool ok = (n0 + j < N) && (k0 + kk < K);
       const double2* src = ok ? R + (long long)(k0 + kk) + (long long)(n0 + j) * t.r_ld : R;
-      cp_async16(&Bs[kk * LDS_B + j], src, ok);
+      cp_async16(&Bs[kk * LDB + j], src, ok);
     }
   } else {
     // op(R)[k][n] = conj(R[n + k*ld]) : contiguous in n
-    const int j = tid & 63;
+    const int j = tid % TN;
 #pragma unroll
-    for (int r = 0; r < 8; ++r) {
-      int kk = (tid >> 6) + 2 * r;
+    for (int r = 0; r < TN * TK / GEMM_THREADS; ++r) {
+      int kk = tid / TN + (GEMM_THREADS / TN) * r;
       bool ok = (n0 + j < N) && (k0 + kk < K);
       const double2* src = ok ? R + (long long)(n0 + j) + (long long)(k0 + kk) * t.r_ld : R;
-      cp_async16(&Bs[kk * LDS_B + j], src, ok);
+      cp_async16(&Bs[kk * LDB + j], src, ok);
     }
   }
 }
 
-__global__ void __launch_bounds__(GEMM_THREADS, 2)
+template <int TM, int TN, int MINB>
+__global__ void __launch_bounds__(GEMM_THREADS, MINB)
 grouped_zgemm_kernel(const GJob* __restrict__ jobs, const GGroup* __restrict__ groups,
                      const GTerm* __restrict__ terms, Bases bases) {
+  constexpr int MI = TM / 16, NI = TN / 16;   // 8x8 MMA sub-tiles per warp (2x2 warps)
+  constexpr int LDS_A = SmemTiles<TM, TN>::LDS_A, LDS_B = SmemTiles<TM, TN>::LDS_B;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  SmemTiles& s = *reinterpret_cast<SmemTiles*>(smem_raw);
+  SmemTiles<TM, TN>& s = *reinterpret_cast<SmemTiles<TM, TN>*>(smem_raw);
   const GJob job = jobs[blockIdx.x];
   const GGroup g = groups[job.group];
   const int m0 = job.tm * TM, n0 = job.tn * TN;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int wm = warp & 1, wn = warp >> 1;
   const int lg = lane >> 2, lt = lane & 3;
+  // The tile's valid 8x8 MMA sub-tiles are split evenly between the 2x2 warps
+  // (warp-uniform counts), so partly filled tiles keep all four SMSPs busy.
+  const int mtot = min(2 * MI, (g.M - m0 + 7) / 8), ntot = min(2 * NI, (g.N - n0 + 7) / 8);
+  const int mh = (mtot + 1) / 2, nh = (ntot + 1) / 2;
+  const int wrow = wm ? mh * 8 : 0, wcol = wn ? nh * 8 : 0;
+  const int mt = wm ? mtot - mh : mh, nt = wn ? ntot - nh : nh;
 
-  double cre[4][4][2], cim[4][4][2];
+  double cre[MI][NI][2], cim[MI][NI][2];
 #pragma unroll
-  for (int a = 0; a < 4; ++a)
+  for (int a = 0; a < MI; ++a)
 #pragma unroll
-    for (int b = 0; b < 4; ++b) {
+    for (int b = 0; b < NI; ++b) {
       cre[a][b][0] = cre[a][b][1] = 0.0;
       cim[a][b][0] = cim[a][b][1] = 0.0;
     }
 
-  for (int ti = g.t0; ti < g.t1; ++ti) {
+  for (int ti = job.t0; ti < job.t1; ++ti) {
     const GTerm t = terms[ti];
     if (t.kind == TK_GEMM) {
       const double2* L = bases.p[t.l_base] + t.l_off;
@@ -141,33 +153,47 @@ grouped_zgemm_kernel(const GJob* __restrict__ jobs, const GGroup* __restrict__ g
         __syncthreads();
         const double2* As = s.a[kt & 1];
         const double2* Bs = s.b[kt & 1];
+        const int krem = t.K - kt * TK;   // k-steps of 4 past K are all zero padding
 #pragma unroll
         for (int kb = 0; kb < TK / 4; ++kb) {
+          if (kb * 4 >= krem) break;
           const int krow = kb * 4 + lt;
-          double ar[4], ai[4], nai[4], br[4], bi[4];
+          double ar[MI], ai[MI], nai[MI], br[NI], bi[NI];
 #pragma unroll
-          for (int mi = 0; mi < 4; ++mi) {
-            double2 v = As[krow * LDS_A + wm * 32 + mi * 8 + lg];
+          for (int mi = 0; mi < MI; ++mi) {
+            double2 v = As[krow * LDS_A + wrow + mi * 8 + lg];
             ar[mi] = v.x;
             ai[mi] = lc ? -v.y : v.y;
             nai[mi] = -ai[mi];
           }
 #pragma unroll
-          for (int ni = 0; ni < 4; ++ni) {
-            double2 v = Bs[krow * LDS_B + wn * 32 + ni * 8 + lg];
+          for (int ni = 0; ni < NI; ++ni) {
+            double2 v = Bs[krow * LDS_B + wcol + ni * 8 + lg];
             double vr = v.x, vi = rc ? -v.y : v.y;
             br[ni] = t.ar * vr - t.ai * vi;
             bi[ni] = t.ar * vi + t.ai * vr;
           }
+          // four passes so the two updates of each accumulator are 32 MMAs apart
 #pragma unroll
-          for (int mi = 0; mi < 4; ++mi)
+          for (int mi = 0; mi < MI; ++mi)
 #pragma unroll
-            for (int ni = 0; ni < 4; ++ni) {
-              dmma(cre[mi][ni][0], cre[mi][ni][1], ar[mi], br[ni]);
-              dmma(cre[mi][ni][0], cre[mi][ni][1], nai[mi], bi[ni]);
-              dmma(cim[mi][ni][0], cim[mi][ni][1], ar[mi], bi[ni]);
-              dmma(cim[mi][ni][0], cim[mi][ni][1], ai[mi], br[ni]);
-            }
+            for (int ni = 0; ni < NI; ++ni)
+              if (mi < mt && ni < nt) dmma(cre[mi][ni][0], cre[mi][ni][1], ar[mi], br[ni]);
+#pragma unroll
+          for (int mi = 0; mi < MI; ++mi)
+#pragma unroll
+            for (int ni = 0; ni < NI; ++ni)
+              if (mi < mt && ni < nt) dmma(cim[mi][ni][0], cim[mi][ni][1], ar[mi], bi[ni]);
+#pragma unroll
+          for (int mi = 0; mi < MI; ++mi)
+#pragma unroll
+            for (int ni = 0; ni < NI; ++ni)
+              if (mi < mt && ni < nt) dmma(cre[mi][ni][0], cre[mi][ni][1], nai[mi], bi[ni]);
+#pragma unroll
+          for (int mi = 0; mi < MI; ++mi)
+#pragma unroll
+            for (int ni = 0; ni < NI; ++ni)
+              if (mi < mt && ni < nt) dmma(cim[mi][ni][0], cim[mi][ni][1], ai[mi], br[ni]);
         }
         __syncthreads();
       }
@@ -175,14 +201,15 @@ grouped_zgemm_kernel(const GJob* __restrict__ jobs, const GGroup* __restrict__ g
       // element-wise terms on the accumulator layout
       const double2* R = bases.p[t.r_base] + t.r_off;
 #pragma unroll
-      for (int mi = 0; mi < 4; ++mi)
+      for (int mi = 0; mi < MI; ++mi)
 #pragma unroll
-        for (int ni = 0; ni < 4; ++ni)
+        for (int ni = 0; ni < NI; ++ni)
 #pragma unroll
           for (int e = 0; e < 2; ++e) {
-            int row = m0 + wm * 32 + mi * 8 + lg;
-            int col = n0 + wn * 32 + ni * 8 + 2 * lt + e;
+            int row = m0 + wrow + mi * 8 + lg;
+            int col = n0 + wcol + ni * 8 + 2 * lt + e;
             int rr = row - t.r0, cc = col - t.c0;
+            if (mi >= mt || ni >= nt) continue;
             if (row >= g.M || col >= g.N || rr < 0 || cc < 0 || rr >= t.rm || cc >= t.rn) continue;
             double vr, vi;
             if (t.kind == TK_AXPY) {
@@ -201,19 +228,22 @@ grouped_zgemm_kernel(const GJob* __restrict__ jobs, const GGroup* __restrict__ g
     }
   }
 
-  double2* C = bases.p[g.c_base] + g.c_off;
+  const bool partial = job.part >= 0;
+  double2* C = partial ? bases.part + job.part_off : bases.p[g.c_base] + g.c_off;
+  const long long ldc = partial ? g.M : g.c_ld;
+  const bool acc_old = !partial && g.beta;
 #pragma unroll
-  for (int mi = 0; mi < 4; ++mi)
+  for (int mi = 0; mi < MI; ++mi)
 #pragma unroll
-    for (int ni = 0; ni < 4; ++ni)
+    for (int ni = 0; ni < NI; ++ni)
 #pragma unroll
       for (int e = 0; e < 2; ++e) {
-        int row = m0 + wm * 32 + mi * 8 + lg;
-        int col = n0 + wn * 32 + ni * 8 + 2 * lt + e;
-        if (row < g.M && col < g.N) {
-          double2* p = C + (long long)row + (long long)col * g.c_ld;
+        int row = m0 + wrow + mi * 8 + lg;
+        int col = n0 + wcol + ni * 8 + 2 * lt + e;
+        if (mi < mt && ni < nt && row < g.M && col < g.N) {
+          double2* p = C + (long long)row + (long long)col * ldc;
           double2 v = make_double2(cre[mi][ni][e], cim[mi][ni][e]);
-          if (g.beta) {
+          if (acc_old) {
             double2 o = *p;
             v.x += o.x;
             v.y += o.y;
@@ -221,6 +251,32 @@ grouped_zgemm_kernel(const GJob* __restrict__ jobs, const GGroup* __restrict__ g
           *p = v;
         }
       }
+}
+
+// C = sum of the partial tiles of a split group in fixed order (+ beta*C_old)
+__global__ void reduce_partials_kernel(const GReduce* __restrict__ reds, const GGroup* __restrict__ groups,
+                                       Bases bases) {
+  const GReduce r = reds[blockIdx.y];
+  const GGroup g = groups[r.group];
+  const long long mn = (long long)g.M * g.N;
+  double2* C = bases.p[g.c_base] + g.c_off;
+  const double2* P = bases.part + r.part_off;
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < mn; e += (long long)gridDim.x * blockDim.x) {
+    double sr = 0.0, si = 0.0;
+    for (int p = 0; p < r.nparts; ++p) {
+      double2 v = P[(long long)p * mn + e];
+      sr += v.x;
+      si += v.y;
+    }
+    const long long row = e % g.M, col = e / g.M;
+    double2* c = C + row + col * g.c_ld;
+    if (g.beta) {
+      double2 o = *c;
+      sr += o.x;
+      si += o.y;
+    }
+    *c = make_double2(sr, si);
+  }
 }
 
 // ---------------------------------------------------------------- vector kernels
@@ -484,17 +540,36 @@ inline int grid_for(long long n) {
 
 }  // namespace
 
-cudaError_t launch_grouped_zgemm(const GJob* jobs, int njobs, const GGroup* groups, const GTerm* terms,
-                                 Bases bases, cudaStream_t st) {
-  if (njobs <= 0) return cudaSuccess;
-  const size_t smem = sizeof(SmemTiles);
+template <int TM, int TN, int MINB>
+cudaError_t launch_tile(const GJob* jobs, int njobs, const GGroup* groups, const GTerm* terms, Bases bases,
+                        cudaStream_t st) {
+  const size_t smem = sizeof(SmemTiles<TM, TN>);
   static bool attr = false;
   if (!attr) {
-    cudaError_t e = cudaFuncSetAttribute(grouped_zgemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = cudaFuncSetAttribute(grouped_zgemm_kernel<TM, TN, MINB>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     attr = true;
   }
-  grouped_zgemm_kernel<<<njobs, GEMM_THREADS, smem, st>>>(jobs, groups, terms, bases);
+  grouped_zgemm_kernel<TM, TN, MINB><<<njobs, GEMM_THREADS, smem, st>>>(jobs, groups, terms, bases);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_grouped_zgemm(const GJob* jobs, int njobs, const GGroup* groups, const GTerm* terms,
+                                 Bases bases, cudaStream_t st, int tile) {
+  if (njobs <= 0) return cudaSuccess;
+  if (tile == 32) return launch_tile<32, 32, 6>(jobs, njobs, groups, terms, bases, st);
+  return launch_tile<64, 64, 2>(jobs, njobs, groups, terms, bases, st);
+}
+
+cudaError_t launch_reduce_partials(const GReduce* reds, int nred, const GGroup* groups, Bases bases,
+                                   long long max_elems, cudaStream_t st) {
+  if (nred <= 0) return cudaSuccess;
+  long long bx = (max_elems + 255) / 256;
+  if (bx > 64) bx = 64;
+  if (bx < 1) bx = 1;
+  dim3 grid((unsigned)bx, (unsigned)nred);
+  reduce_partials_kernel<<<grid, 256, 0, st>>>(reds, groups, bases);
   return cudaGetLastError();
 }
 

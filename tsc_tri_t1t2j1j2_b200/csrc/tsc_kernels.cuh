@@ -35,18 +35,32 @@ struct GGroup {
   uint8_t c_base, beta, pad0, pad1;
 };
 
+// One CTA's work: tile (tm, tn) of a group over terms [t0, t1).  part < 0 writes
+// the group's output; otherwise the tile is a partial sum written to the partial
+// buffer at part_off (ld = group M) and reduced by launch_reduce_partials.
 struct GJob {
-  int group, tm, tn, pad;
+  int group, tm, tn, t0, t1, part;
+  long long part_off;
+};
+
+// Partial sums of one split group: C = sum_{p<nparts} P[p] + beta*C_old.
+struct GReduce {
+  int group, nparts;
+  long long part_off;   // first partial; partial p at part_off + p*M*N
 };
 
 struct Bases {
   double2* p[4];
+  double2* part;
 };
 
-constexpr int GEMM_TM = 64, GEMM_TN = 64, GEMM_TK = 16, GEMM_THREADS = 128;
+constexpr int GEMM_TK = 16, GEMM_THREADS = 128;
 
+// tile = CTA output tile edge (64: 64x64, 2 CTAs/SM; 32: 32x32, 6 CTAs/SM)
 cudaError_t launch_grouped_zgemm(const GJob* jobs, int njobs, const GGroup* groups, const GTerm* terms,
-                                 Bases bases, cudaStream_t st);
+                                 Bases bases, cudaStream_t st, int tile);
+cudaError_t launch_reduce_partials(const GReduce* reds, int nred, const GGroup* groups, Bases bases,
+                                   long long max_elems, cudaStream_t st);
 
 // ---- vector kernels (Lanczos, eigen.f90 / block.f90:1092-1354) -------------------
 // partial sums of Re<x_j, y> for j < nvec (x_j = X + j*ld), deterministic two-pass
