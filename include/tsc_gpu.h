@@ -150,6 +150,20 @@ int tsc_hpsi_stats(tsc_ctx* ctx, double* device_ms, double* ref_flops, double* e
  * enqueued on it, so callers can order their own work and time it with events. */
 void* tsc_stream(tsc_ctx* ctx);
 
+/* H.psi on device pointers that allocates nothing (no counterpart in the
+ * reference).  For callers that cannot call cudaMalloc or any allocating
+ * library routine when they need H.psi (a host that owns the whole device
+ * memory budget through its own pool, an iteration that must not change the
+ * allocation state).  Same result as tsc_hpsi_device, enqueued on the context
+ * stream; its scratch is one fixed array of TSC_NOALLOC_SCRATCH_ELEMS complex128
+ * elements (64 MiB) in device global memory, held by every GPU that loads the
+ * library until exit.  Superblocks needing more scratch are rejected with
+ * TSC_E_LIMIT.  The first call on a device resolves the array's address (make
+ * it before any stream capture).  All calls share the array: calls that
+ * overlap on the GPU race. */
+#define TSC_NOALLOC_SCRATCH_ELEMS 4194304LL
+int tsc_hpsi_noalloc(tsc_ctx* ctx, const void* d_in, void* d_out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -19,7 +19,7 @@ EXPORTED = [
     "tsc_create", "tsc_destroy", "tsc_last_error", "tsc_tot_num_up", "tsc_superblock_set",
     "tsc_superblock_dim", "tsc_hpsi", "tsc_hpsi_device", "tsc_lanczos", "tsc_truncate",
     "tsc_renormalize", "tsc_wave_transform", "tsc_dmrg_run", "tsc_set_capture", "tsc_get_capture",
-    "tsc_hpsi_stats", "tsc_stream",
+    "tsc_hpsi_stats", "tsc_stream", "tsc_hpsi_noalloc",
 ]
 
 
@@ -81,6 +81,7 @@ def load():
     L.tsc_hpsi_stats.argtypes = [c_void, pd, pd, pd, pi]
     L.tsc_stream.argtypes = [c_void]
     L.tsc_stream.restype = c_void
+    L.tsc_hpsi_noalloc.argtypes = [c_void, c_void, c_void]
     _lib = L
     return L
 

@@ -5,17 +5,10 @@
 #include <memory>
 
 #include "../../include/tsc_gpu.h"
+#include "tsc_ctx.hpp"
 #include "tsc_engine.hpp"
 
 using namespace tsc;
-
-struct tsc_ctx {
-  std::unique_ptr<Engine> eng;
-  std::string err;
-  std::vector<int> out_ints;
-  std::vector<cplx> out_data;
-  int device = 0;
-};
 
 namespace {
 

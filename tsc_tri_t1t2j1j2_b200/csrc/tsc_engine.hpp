@@ -148,6 +148,7 @@ struct TaskList {
   int tile = 64;           // CTA tile edge used for this list (64 or 32)
   long long max_red_elems = 0;
   DevBufP part;            // partial tiles of split groups
+  long long part_elems = 0;
   double exec_flops = 0;   // flops the kernel executes
   long long nterms = 0;
   int add_group(double2* abs_c, uint8_t base, long long c_off, int ld, int M, int N, int beta);

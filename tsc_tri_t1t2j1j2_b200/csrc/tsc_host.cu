@@ -390,7 +390,7 @@ void TaskList::upload(cudaStream_t st, int slots, int waves) {
       total += c * (long long)((g.M + TMt - 1) / TMt) * ((g.N + TNt - 1) / TNt);
   }
   const long long target = std::max<long long>(8, total / std::max(1, slots * waves));
-  long long part_elems = 0;
+  part_elems = 0;
   // pass 2: jobs, splitting long groups into term chunks of about `target`
   for (size_t gi = 0; gi < groups.size(); ++gi) {
     const GGroup& g = groups[gi];

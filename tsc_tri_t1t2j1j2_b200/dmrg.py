@@ -103,6 +103,11 @@ class Context:
         """H.psi on device pointers (e.g. torch tensors' data_ptr()), enqueued on the context stream."""
         self._check(self.L.tsc_hpsi_device(self.h, ctypes.c_void_p(d_in), ctypes.c_void_p(d_out)))
 
+    def hpsi_noalloc(self, d_in: int, d_out: int):
+        """H.psi on device pointers that allocates nothing (scratch: a fixed 64 MiB
+        device array shared by all calls; see include/tsc_gpu.h)."""
+        self._check(self.L.tsc_hpsi_noalloc(self.h, ctypes.c_void_p(d_in), ctypes.c_void_p(d_out)))
+
     @property
     def stream(self) -> int:
         """cudaStream_t of this context (device-pointer calls are enqueued on it)."""
