@@ -320,9 +320,11 @@ def run_gpu(args):
     return 0
 
 
-# bytes the dominant kernel moves per H.psi (dram read + write), from ncu on this
-# workload (profiles/hpsi_grouped_zgemm_yc4x12_m1000.md); None until captured
-TRAFFIC_BYTES_PER_STEP = None
+# bytes the dominant kernel moves per H.psi (dram__bytes_read.sum + dram__bytes_write.sum
+# of its two launches), from one ncu capture of this workload
+# (profiles/hpsi_grouped_zgemm_yc4x12_m1000.md): phase 1 0.0917 + 0.3857 GB,
+# phase 2 1.3513 + 0.0816 GB
+TRAFFIC_BYTES_PER_STEP = 1.9103e9
 
 
 def main():
