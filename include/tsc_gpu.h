@@ -68,6 +68,10 @@ typedef struct tsc_step_log {
   double hpsi_seconds;     /* device time of the H.psi launches of this solve */
   double hpsi_flops;       /* algorithmic flops (reference association order) */
   double step_seconds;     /* wall time of the whole DMRG step on the device */
+  /* wall time of the step's parts: superblock set-up (hmerge + task lists),
+   * Lanczos (H.psi included), density matrix + truncation, block growth +
+   * renormalisation, wave transformation */
+  double set_seconds, lanczos_seconds, truncate_seconds, grow_seconds, wave_seconds;
 } tsc_step_log;
 
 typedef struct tsc_ctx tsc_ctx;

@@ -38,7 +38,9 @@ class StepLog(ctypes.Structure):
     _fields_ = [("phase", c_int), ("sys_len", c_int), ("env_len", c_int), ("e0", c_double),
                 ("lanczos_iters", c_int), ("num_state", c_int), ("trun_err", c_double), ("entropy", c_double),
                 ("entropy_mult", c_double), ("hpsi_calls", c_int), ("hpsi_seconds", c_double),
-                ("hpsi_flops", c_double), ("step_seconds", c_double)]
+                ("hpsi_flops", c_double), ("step_seconds", c_double), ("set_seconds", c_double),
+                ("lanczos_seconds", c_double), ("truncate_seconds", c_double), ("grow_seconds", c_double),
+                ("wave_seconds", c_double)]
 
 
 class TscError(RuntimeError):

@@ -349,7 +349,9 @@ int tsc_dmrg_run(tsc_ctx* ctx, const tsc_sweep_config* sw, tsc_step_log* log, in
     for (int i = 0; i < nsteps && i < max_steps && log; ++i) {
       const auto& s = recs[i];
       log[i] = tsc_step_log{s.phase, s.sys_len, s.env_len, s.e0, s.iters, s.num_state, s.err, s.ent, s.ent_mult,
-                            s.hpsi_calls, s.hpsi_seconds, s.hpsi_flops, s.step_seconds};
+                            s.hpsi_calls, s.hpsi_seconds, s.hpsi_flops, s.step_seconds,
+                            s.set_seconds, s.lanczos_seconds, s.truncate_seconds, s.grow_seconds,
+                            s.wave_seconds};
     }
   });
   return rc == TSC_OK ? nsteps : rc;

@@ -11,30 +11,120 @@
 #include <cmath>
 #include <cstring>
 
+#include <condition_variable>
+#include <functional>
+#include <mutex>
+#include <thread>
+
 #include "tsc_engine.hpp"
 
 namespace tsc {
+
+// Phase timer of the step records: wall clock after the engine stream drains.
+static inline std::chrono::steady_clock::time_point phase_clock(cudaStream_t st) {
+  cuda_check(cudaStreamSynchronize(st), "sync");
+  return std::chrono::steady_clock::now();
+}
+static inline double secs(std::chrono::steady_clock::time_point a, std::chrono::steady_clock::time_point b) {
+  return std::chrono::duration<double>(b - a).count();
+}
+
+
+// Per-sector zheevd calls are independent and each occupies a small part of the
+// GPU, but cuSOLVER's zheevd waits on the host inside the call.  So each lane is
+// a host thread with its own stream, cuSOLVER handle and workspace; the engine
+// stream forks to the lanes through an event and joins their done events.
+struct Engine::EigLanes {
+  struct Lane {
+    cudaStream_t s = nullptr;
+    cusolverDnHandle_t h = nullptr;
+    cudaEvent_t done = nullptr;
+    DevBufP work;
+    int lwork = 0;
+    std::thread th;
+  };
+  std::vector<Lane> lane;
+  cudaEvent_t fork = nullptr;
+  std::mutex mu;
+  std::condition_variable cv_go, cv_done;
+  std::function<void(int)> task;
+  long long gen = 0;
+  int pending = 0;
+  bool stop = false;
+  std::string err;
+
+  EigLanes(int n, int device) : lane(n) {
+    cuda_check(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming), "cudaEventCreate");
+    for (auto& l : lane) {
+      cuda_check(cudaStreamCreateWithFlags(&l.s, cudaStreamNonBlocking), "cudaStreamCreate");
+      cuda_check(cudaEventCreateWithFlags(&l.done, cudaEventDisableTiming), "cudaEventCreate");
+      if (cusolverDnCreate(&l.h) != CUSOLVER_STATUS_SUCCESS) throw Error(-3, "cusolverDnCreate failed");
+      if (cusolverDnSetStream(l.h, l.s) != CUSOLVER_STATUS_SUCCESS) throw Error(-3, "cusolverDnSetStream failed");
+    }
+    for (int i = 0; i < n; ++i)
+      lane[i].th = std::thread([this, i, device] {
+        cudaSetDevice(device);
+        long long seen = 0;
+        while (true) {
+          std::function<void(int)> t;
+          {
+            std::unique_lock<std::mutex> lk(mu);
+            cv_go.wait(lk, [&] { return stop || gen != seen; });
+            if (stop) return;
+            seen = gen;
+            t = task;
+          }
+          std::string e;
+          try {
+            t(i);
+          } catch (std::exception& x) {
+            e = x.what();
+          }
+          std::lock_guard<std::mutex> lk(mu);
+          if (!e.empty() && err.empty()) err = e;
+          if (--pending == 0) cv_done.notify_all();
+        }
+      });
+  }
+  // runs f(lane) on every lane thread and waits for all of them
+  void run(std::function<void(int)> f) {
+    std::unique_lock<std::mutex> lk(mu);
+    task = std::move(f);
+    err.clear();
+    pending = (int)lane.size();
+    gen++;
+    cv_go.notify_all();
+    cv_done.wait(lk, [&] { return pending == 0; });
+    if (!err.empty()) throw Error(-3, err);
+  }
+  ~EigLanes() {
+    {
+      std::lock_guard<std::mutex> lk(mu);
+      stop = true;
+    }
+    cv_go.notify_all();
+    for (auto& l : lane)
+      if (l.th.joinable()) l.th.join();
+    for (auto& l : lane) {
+      if (l.s) cudaStreamSynchronize(l.s);
+      l.work.reset();
+      release_stream_cache(l.s);
+      if (l.s) cudaStreamSynchronize(l.s);
+      if (l.h) cusolverDnDestroy(l.h);
+      if (l.done) cudaEventDestroy(l.done);
+      if (l.s) cudaStreamDestroy(l.s);
+    }
+    if (fork) cudaEventDestroy(fork);
+  }
+};
+constexpr int kEigLanes = 8;
 
 namespace {
 inline double pm1(int e) { return ((e % 2) + 2) % 2 == 0 ? 1.0 : -1.0; }
 inline long long absoff(const double2* p) { return (long long)((uintptr_t)p / sizeof(double2)); }
 
-struct Solver {
-  cusolverDnHandle_t h = nullptr;
-  Solver() {
-    if (cusolverDnCreate(&h) != CUSOLVER_STATUS_SUCCESS) throw Error(-3, "cusolverDnCreate failed");
-  }
-  ~Solver() {
-    if (h) cusolverDnDestroy(h);
-  }
-};
-Solver& solver() {
-  static thread_local Solver s;
-  return s;
-}
-
 // scalar slots in d_scal
-constexpr int S_ALPHA = 0, S_BETA = 128, S_UV = 256, S_UU = 384, S_RES = 512, S_Z = 520, S_N2 = 700;
+constexpr int S_ALPHA = 0, S_BETA = 128, S_UV = 256, S_UU = 384, S_RES = 512, S_Z = 520, S_N2 = 700, S_PKT = 704;
 
 // Density-matrix eigenvalues below this are rounding noise (rho has unit trace).
 constexpr double kZeroWeight = 1e-13;
@@ -106,82 +196,79 @@ void Engine::lanczos(double2* d_psi, double lanzero, int* iters, double* e0, dou
   int nblk = (int)((n + 8191) / 8192);
   DevBuf part((size_t)((long long)nblk * (loop_in + 2) + 1) / 2 + 1, st, false);
   double* d_part = reinterpret_cast<double*>(part.p);
-  double* a_d = d_scal + S_ALPHA;
+  double* a_d = d_scal + S_ALPHA;   // alpha_j at a_d[j], beta_j at b_d[j] (1-based, as eigen.f90)
   double* b_d = d_scal + S_BETA;
   double* uv_d = d_scal + S_UV;
   double* uu_d = d_scal + S_UU;
-  std::vector<double> alpha(loop_in + 2, 0.0), beta(loop_in + 2, 0.0);
   double lastmin = 1024.0, ritzmin = 0.0;
   int iter_out = 0, last = 1;
-  float hms = 0.f;
   int calls = 0;
+  // H.psi launches are bracketed by events that are read once, after the solve
   auto do_hpsi = [&](int j) {
-    hpsi(v(j), v(j + 1));
-    calls++;
-    cuda_check(cudaEventSynchronize(ev1), "event sync");
-    float ms = 0.f;
-    cudaEventElapsedTime(&ms, ev0, ev1);
-    hms += ms;
-  };
-  auto rd = [&](int slot) {
-    cuda_check(cudaMemcpyAsync(h_scal + slot, d_scal + slot, sizeof(double), cudaMemcpyDeviceToHost, st), "d2h");
-    cuda_check(cudaStreamSynchronize(st), "sync");
-    return h_scal[slot];
-  };
-  auto tridiag = [&](int m, bool vec) {
-    for (int k = 1; k <= m; ++k) {
-      h_scal[1024 + k - 1] = alpha[k];
-      h_scal[1024 + 128 + k - 1] = beta[k];
+    if ((size_t)(2 * calls + 2) > hpsi_events.size()) {
+      for (int q = 0; q < 2; ++q) {
+        cudaEvent_t e;
+        cuda_check(cudaEventCreate(&e), "cudaEventCreate");
+        hpsi_events.push_back(e);
+      }
     }
-    cuda_check(cudaMemcpyAsync(d_scal + 1024, h_scal + 1024, 256 * sizeof(double), cudaMemcpyHostToDevice, st), "h2d");
-    cuda_check(launch_tridiag_lowest(d_scal + 1024, d_scal + 1024 + 128, m, vec ? 1 : 0, d_scal + S_RES, d_scal + S_Z, st),
-               "tridiag");
-    cuda_check(cudaMemcpyAsync(h_scal + S_RES, d_scal + S_RES, (vec ? 1 + 128 : 1) * sizeof(double),
-                               cudaMemcpyDeviceToHost, st),
-               "d2h");
+    cuda_check(cudaEventRecord(hpsi_events[2 * calls], st), "event");
+    hpsi(v(j), v(j + 1));
+    cuda_check(cudaEventRecord(hpsi_events[2 * calls + 1], st), "event");
+    calls++;
+  };
+  auto read_back = [&](int slot, int count) {
+    cuda_check(cudaMemcpyAsync(h_scal + slot, d_scal + slot, count * sizeof(double), cudaMemcpyDeviceToHost, st), "d2h");
     cuda_check(cudaStreamSynchronize(st), "sync");
+  };
+  // lowest eigenpair of T_m (alpha_1..m, beta_1..m-1) from the device slots
+  auto tridiag_vec = [&](int m) {
+    cuda_check(launch_tridiag_lowest(a_d + 1, b_d + 1, m, 1, d_scal + S_RES, d_scal + S_Z, st), "tridiag");
+    read_back(S_RES, 1);
     return h_scal[S_RES];
   };
   bool done = false;
   while (iter_out <= loop_out && !done) {
     iter_out++;
     last = 1;
-    std::fill(alpha.begin(), alpha.end(), 0.0);
-    std::fill(beta.begin(), beta.end(), 0.0);
     ritzmin = lastmin;
     cuda_check(cudaMemcpyAsync(v(1), d_psi, n * sizeof(double2), cudaMemcpyDeviceToDevice, st), "copy");
     normalize(v(1), n);
     cuda_check(launch_multi_dot(v(1), ld, 1, v(1), n, d_part, uu_d + 1, st), "uu");
     do_hpsi(1);
     cuda_check(launch_multi_dot(v(1), ld, 1, v(2), n, d_part, a_d + 1, st), "alpha");
-    alpha[1] = rd(S_ALPHA + 1);
-    ritzmin = alpha[1];
+    read_back(S_ALPHA + 1, 1);
+    ritzmin = h_scal[S_ALPHA + 1];
     bool conv = false;
     while (last < loop_in) {
+      // One iteration runs on the device without a host decision; the host
+      // reads {ritz of T_(last+1), |w|^2, alpha_(last+1)} once at its end.  The
+      // reference stops before the Gram-Schmidt step when beta_last <= lanzero
+      // (eigen.f90:70-74); here that test is applied to the read-back value and
+      // the iteration's remaining work (vectors last+1, last+2 and slots last+1)
+      // is discarded, which leaves the same state.
       double2* w = v(last + 1);
       cuda_check(launch_lanczos_update(w, v(last), last >= 2 ? v(last - 1) : nullptr, a_d + last,
                                        b_d + (last >= 2 ? last - 1 : 0), n, st),
                  "update");
       cuda_check(launch_multi_dot(w, ld, 1, w, n, d_part, d_scal + S_N2, st), "norm");
-      double n2 = rd(S_N2);
-      beta[last] = std::sqrt(n2);
-      h_scal[S_BETA + last] = beta[last];
-      cuda_check(cudaMemcpyAsync(b_d + last, h_scal + S_BETA + last, sizeof(double), cudaMemcpyHostToDevice, st), "h2d");
-      if (std::fabs(beta[last]) <= lanzero) {
-        conv = true;
-        break;
-      }
       cuda_check(launch_scale(w, d_scal + S_N2, n, 1, st), "normalize");
       // Gram_Schmidt_process against v(1..last) (block.f90:1251-1289)
       cuda_check(launch_multi_dot(v(1), ld, last, w, n, d_part, uv_d + 1, st), "uv");
       cuda_check(launch_gs_subtract(w, v(1), ld, last, uv_d + 1, uu_d + 1, n, st), "gs");
       normalize(w, n);
       cuda_check(launch_multi_dot(w, ld, 1, w, n, d_part, uu_d + last + 1, st), "uu");
+      do_hpsi(last + 1);
+      cuda_check(launch_multi_dot(v(last + 1), ld, 1, v(last + 2), n, d_part, a_d + last + 1, st), "alpha");
+      cuda_check(launch_lanczos_tail(d_scal + S_N2, a_d, b_d, last + 1, d_scal + S_RES, d_scal + S_PKT, st), "tail");
+      read_back(S_PKT, 3);
+      const double beta_last = std::sqrt(h_scal[S_PKT + 1]);
+      if (std::fabs(beta_last) <= lanzero) {
+        conv = true;
+        break;
+      }
       last++;
-      do_hpsi(last);
-      cuda_check(launch_multi_dot(v(last), ld, 1, v(last + 1), n, d_part, a_d + last, st), "alpha");
-      alpha[last] = rd(S_ALPHA + last);
-      double d0 = tridiag(last, false);
+      const double d0 = h_scal[S_PKT];
       if (std::fabs(d0 - ritzmin) <= lanzero || (last == loop_in && iter_out == loop_out)) {
         ritzmin = d0;
         lastmin = ritzmin;
@@ -196,16 +283,22 @@ void Engine::lanczos(double2* d_psi, double lanzero, int* iters, double* e0, dou
       break;
     }
     // restart (eigen.f90:114-129)
-    ritzmin = tridiag(last, true);
+    ritzmin = tridiag_vec(last);
     lastmin = ritzmin;
     cuda_check(launch_combine(d_psi, v(1), ld, last, d_scal + S_Z, n, st), "combine");
     normalize(d_psi, n);
   }
   // eigen.f90:137-156
-  ritzmin = tridiag(last, true);
+  ritzmin = tridiag_vec(last);
   cuda_check(launch_combine(d_psi, v(1), ld, last, d_scal + S_Z, n, st), "combine");
   normalize(d_psi, n);
   cuda_check(cudaStreamSynchronize(st), "sync");
+  double hms = 0.0;
+  for (int c = 0; c < calls; ++c) {
+    float ms = 0.f;
+    cuda_check(cudaEventElapsedTime(&ms, hpsi_events[2 * c], hpsi_events[2 * c + 1]), "event time");
+    hms += ms;
+  }
   *iters = (iter_out - 1) * loop_in + last;
   *e0 = ritzmin;
   if (hpsi_ms) *hpsi_ms = hms;
@@ -253,36 +346,60 @@ void Engine::truncate(int side, const double2* d_psi, const WLayout& wl, int kep
   }
   tl.upload(st);
   run_tasks(tl, w.p, nullptr, nullptr);
-  // zheev per sector (den_mat.f90:243): cuSOLVER zheevd, eigenvalues ascending
-  cusolverDnHandle_t h = solver().h;
-  cusolverDnSetStream(h, st);
-  int dim = 0, maxd = 0;
+  // zheev per sector (den_mat.f90:243): cuSOLVER zheevd, eigenvalues ascending.
+  // Sectors are dealt to the lanes largest first, each to the least loaded lane.
+  int dim = 0;
+  std::vector<int> eoffs(wl.num);
   for (int k = 0; k < wl.num; ++k) {
-    int d = side == 0 ? wl.sec[k].sys_dim : wl.sec[k].env_dim;
-    dim += d;
-    maxd = std::max(maxd, d);
+    eoffs[k] = dim;
+    dim += side == 0 ? wl.sec[k].sys_dim : wl.sec[k].env_dim;
   }
   DevBuf ev((size_t)(dim + 2) / 2 + 1, st, false);
   double* d_ev = reinterpret_cast<double*>(ev.p);
-  int lwork = 0;
-  if (maxd > 0 &&
-      cusolverDnZheevd_bufferSize(h, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, maxd,
-                                  reinterpret_cast<cuDoubleComplex*>(den->p), maxd, d_ev, &lwork) !=
-          CUSOLVER_STATUS_SUCCESS)
-    throw Error(-3, "zheevd buffer size");
-  DevBuf work((size_t)std::max(lwork, 1) + 1, st, false);
-  DevBuf info(1, st, true);
-  int eoff = 0;
-  for (int k = 0; k < wl.num; ++k) {
-    int d = side == 0 ? wl.sec[k].sys_dim : wl.sec[k].env_dim;
-    if (d > 0 &&
-        cusolverDnZheevd(h, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, d,
-                         reinterpret_cast<cuDoubleComplex*>(den->p + doff[k]), d, d_ev + eoff,
-                         reinterpret_cast<cuDoubleComplex*>(work.p), lwork,
-                         reinterpret_cast<int*>(info.p)) != CUSOLVER_STATUS_SUCCESS)
-      throw Error(-3, "zheevd");
-    eoff += d;
+  DevBuf info((size_t)(wl.num + 1) / 4 + 1, st, true);   // one int per sector
+  int* d_info = reinterpret_cast<int*>(info.p);
+  if (!eig) eig = std::make_shared<EigLanes>(kEigLanes, device_);
+  std::vector<int> order(wl.num);
+  for (int k = 0; k < wl.num; ++k) order[k] = k;
+  auto sdim = [&](int k) { return side == 0 ? wl.sec[k].sys_dim : wl.sec[k].env_dim; };
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return sdim(a) > sdim(b); });
+  std::vector<std::vector<int>> mine(kEigLanes);
+  std::vector<double> load(kEigLanes, 0.0);
+  for (int k : order) {
+    if (sdim(k) <= 0) continue;
+    int l = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+    mine[l].push_back(k);
+    double d = sdim(k);
+    load[l] += d * d * d + 2.0e5;   // O(d^3) work plus a fixed launch cost
   }
+  cuda_check(cudaEventRecord(eig->fork, st), "event");
+  EigLanes* E = eig.get();
+  eig->run([&](int l) {
+    if (mine[l].empty()) return;
+    auto& L = E->lane[l];
+    cuda_check(cudaStreamWaitEvent(L.s, E->fork, 0), "wait");
+    const int maxd = sdim(mine[l].front());
+    int lwork = 0;
+    if (cusolverDnZheevd_bufferSize(L.h, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, maxd,
+                                    reinterpret_cast<cuDoubleComplex*>(den->p), maxd, d_ev, &lwork) !=
+        CUSOLVER_STATUS_SUCCESS)
+      throw Error(-3, "zheevd buffer size");
+    if (lwork > L.lwork) {
+      L.work = std::make_shared<DevBuf>((size_t)lwork + 1, L.s, false);
+      L.lwork = lwork;
+    }
+    for (int k : mine[l]) {
+      const int d = sdim(k);
+      if (cusolverDnZheevd(L.h, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, d,
+                           reinterpret_cast<cuDoubleComplex*>(den->p + doff[k]), d, d_ev + eoffs[k],
+                           reinterpret_cast<cuDoubleComplex*>(L.work->p), L.lwork, d_info + k) !=
+          CUSOLVER_STATUS_SUCCESS)
+        throw Error(-3, "zheevd");
+    }
+    cuda_check(cudaEventRecord(L.done, L.s), "event");
+  });
+  for (int l = 0; l < kEigLanes; ++l)
+    if (!mine[l].empty()) cuda_check(cudaStreamWaitEvent(st, eig->lane[l].done, 0), "wait");
   // canonical eigenvector phases (see launch_phase_fix)
   for (int k = 0; k < wl.num; ++k) {
     int d = side == 0 ? wl.sec[k].sys_dim : wl.sec[k].env_dim;
@@ -290,10 +407,11 @@ void Engine::truncate(int side, const double2* d_psi, const WLayout& wl, int kep
   }
   std::vector<double> evh(dim + 1);
   if (dim) cuda_check(cudaMemcpyAsync(evh.data() + 1, d_ev, dim * sizeof(double), cudaMemcpyDeviceToHost, st), "d2h");
-  int infoh = 0;
-  cuda_check(cudaMemcpyAsync(&infoh, info.p, sizeof(int), cudaMemcpyDeviceToHost, st), "d2h");
+  std::vector<int> infoh(wl.num, 0);
+  if (wl.num) cuda_check(cudaMemcpyAsync(infoh.data(), d_info, wl.num * sizeof(int), cudaMemcpyDeviceToHost, st), "d2h");
   cuda_check(cudaStreamSynchronize(st), "sync");
-  if (infoh != 0) throw Error(-3, "zheevd did not converge");
+  for (int k = 0; k < wl.num; ++k)
+    if (infoh[k] != 0) throw Error(-3, "zheevd did not converge");
   // eigenvalues at rounding-noise level count as exact zeros (null_completion)
   for (int i = 1; i <= dim; ++i)
     if (evh[i] < kZeroWeight) evh[i] = 0.0;
@@ -1099,11 +1217,16 @@ void Engine::lanczos_step(int phase, DModel& sys, DModel& env, const Basis& sys_
   rec.phase = phase;
   rec.sys_len = sys.len;
   rec.env_len = env.len;
+  auto t0 = phase_clock(st);
   superblock_set(DModel(sys), DModel(env), Basis(sys_bs), Basis(env_bs), WLayout(wl));
+  auto t1 = phase_clock(st);
+  rec.set_seconds = secs(t0, t1);
   if (nsolve_ == capture_step) capture_superblock(psi);
   double hms = 0;
   int calls = 0;
+  t1 = phase_clock(st);
   lanczos(psi->p, lanzero_, &rec.iters, &rec.e0, &hms, &calls);
+  rec.lanczos_seconds = secs(t1, phase_clock(st));
   rec.hpsi_calls = calls;
   rec.hpsi_seconds = hms * 1e-3;
   rec.hpsi_flops = sb.ref_flops * calls;
@@ -1153,6 +1276,7 @@ void Engine::warm_up(int end_id, double trun_err, std::vector<StepRec>* log) {
       return t;
     };
     TruncResult sr, er;
+    auto tp = phase_clock(st);
     if (sys_bs.dim <= kept_max_) {
       sr.trun = ident(sys_bs);
       sr.num_state = sys_bs.dim;
@@ -1163,10 +1287,17 @@ void Engine::warm_up(int end_id, double trun_err, std::vector<StepRec>* log) {
     rec.err = sr.err;
     rec.ent = sr.ent;
     rec.ent_mult = sr.ent_mult;
+    auto tq = phase_clock(st);
+    rec.truncate_seconds += secs(tp, tq);
     grow(0, sys, sys_bs, sr.trun, 0);
+    tp = phase_clock(st);
+    rec.grow_seconds += secs(tq, tp);
     if (env_bs.dim <= kept_max_) er.trun = ident(env_bs);
     else truncate(1, psi->p, wl, kept_min_, kept_max_, trun_err, er);
+    tq = phase_clock(st);
+    rec.truncate_seconds += secs(tp, tq);
     grow(1, env, env_bs, er.trun, sys.len);
+    rec.grow_seconds += secs(tq, phase_clock(st));
     sys_models[label + 1] = sys;
     env_models[label + 1] = env;
     sys_truns[label + 1] = sr.trun;
@@ -1193,6 +1324,7 @@ void Engine::left_to_right(int bg_id, int end_id, double trun_err, std::vector<S
   bool first = true;
   while (true) {
     auto t0 = std::chrono::steady_clock::now();
+    double wave_s = 0.0;
     if (!first) {
       if (!(label + 1 <= end_id)) break;
       sys_bs = get_basis(sys.ham);
@@ -1203,7 +1335,9 @@ void Engine::left_to_right(int bg_id, int end_id, double trun_err, std::vector<S
       WLayout nl = get_super(sys_bs, env_bs, tot_num_up, tot_num_down);
       env_trun = env_truns.at(N - label - 1);
       DevBufP np = std::make_shared<DevBuf>((size_t)std::max<long long>(nl.dim, 1), st, false);
+      auto tw = phase_clock(st);
       wave_trans(0, sys_bs, env_basis, sys_trun, env_trun, wl, psi->p, nl, np->p);
+      wave_s = secs(tw, phase_clock(st));
       wl = nl;
       psi = np;
     } else {
@@ -1218,17 +1352,22 @@ void Engine::left_to_right(int bg_id, int end_id, double trun_err, std::vector<S
       }
     }
     StepRec rec{};
+    rec.wave_seconds = wave_s;
     lanczos_step(1, sys, env, sys_bs, env_bs, wl, psi, rec);
     disk_layout = wl;
     disk_wave = psi;
     TruncResult tr;
+    auto tp = phase_clock(st);
     truncate(0, psi->p, wl, kept_min_, kept_max_, trun_err, tr);
     sys_trun = tr.trun;
     rec.num_state = tr.num_state;
     rec.err = tr.err;
     rec.ent = tr.ent;
     rec.ent_mult = tr.ent_mult;
+    auto tq = phase_clock(st);
+    rec.truncate_seconds = secs(tp, tq);
     grow(0, sys, sys_bs, sys_trun, 0);
+    rec.grow_seconds = secs(tq, phase_clock(st));
     sys_models[label + 1] = sys;
     sys_truns[label + 1] = sys_trun;
     sys_bsm[label + 1] = sys_bs;
@@ -1251,6 +1390,7 @@ void Engine::right_to_left(int bg_id, int end_id, double trun_err, std::vector<S
   bool first = true;
   while (true) {
     auto t0 = std::chrono::steady_clock::now();
+    double wave_s = 0.0;
     if (!first) {
       if (!(label - 1 >= end_id)) break;
       sys_bs = sys_bsm.at(label);
@@ -1261,7 +1401,9 @@ void Engine::right_to_left(int bg_id, int end_id, double trun_err, std::vector<S
       L.setup(sys.ham.len, env.ham.len);
       sys_trun = sys_truns.at(label);
       DevBufP np = std::make_shared<DevBuf>((size_t)std::max<long long>(nl.dim, 1), st, false);
+      auto tw = phase_clock(st);
       wave_trans(1, sys_basis, env_bs, sys_trun, env_trun, wl, psi->p, nl, np->p);
+      wave_s = secs(tw, phase_clock(st));
       wl = nl;
       psi = np;
     } else {
@@ -1276,17 +1418,22 @@ void Engine::right_to_left(int bg_id, int end_id, double trun_err, std::vector<S
       }
     }
     StepRec rec{};
+    rec.wave_seconds = wave_s;
     lanczos_step(2, sys, env, sys_bs, env_bs, wl, psi, rec);
     disk_layout = wl;
     disk_wave = psi;
     TruncResult tr;
+    auto tp = phase_clock(st);
     truncate(1, psi->p, wl, kept_min_, kept_max_, trun_err, tr);
     env_trun = tr.trun;
     rec.num_state = tr.num_state;
     rec.err = tr.err;
     rec.ent = tr.ent;
     rec.ent_mult = tr.ent_mult;
+    auto tq = phase_clock(st);
+    rec.truncate_seconds = secs(tp, tq);
     grow(1, env, env_bs, env_trun, sys.len + 1);
+    rec.grow_seconds = secs(tq, phase_clock(st));
     env_models[N - label] = env;
     env_truns[N - label] = env_trun;
     env_bsm[N - label] = env_bs;

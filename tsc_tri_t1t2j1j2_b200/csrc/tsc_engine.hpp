@@ -30,9 +30,14 @@ struct Error : std::runtime_error {
 void cuda_check(cudaError_t e, const char* what);
 
 // ---- device memory -----------------------------------------------------------
+// Device buffer of complex elements, stream-ordered on `st`.  Buffers are carved
+// from per-stream arenas (chunks of the device pool, best fit, coalesced on
+// free), so a DMRG step makes no driver calls once its arena has grown;
+// release_stream_cache() hands a stream's chunks back to the pool.
 struct DevBuf {
   double2* p = nullptr;
   size_t n = 0;   // complex elements
+  size_t cls = 0; // bytes of the arena block behind p
   cudaStream_t st = nullptr;
   DevBuf() = default;
   DevBuf(size_t count, cudaStream_t s, bool zero);
@@ -41,6 +46,8 @@ struct DevBuf {
   DevBuf& operator=(const DevBuf&) = delete;
 };
 using DevBufP = std::shared_ptr<DevBuf>;
+cudaMemPool_t device_pool();   // the current device's buffer pool
+void release_stream_cache(cudaStream_t s);   // free the cached blocks of stream s
 
 // ---- data model ----------------------------------------------------------------
 struct SubDesc {
@@ -170,6 +177,10 @@ class Engine {
 
   cudaStream_t st = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  std::vector<cudaEvent_t> hpsi_events;   // per-call H.psi brackets of a Lanczos solve
+  int device_ = 0;
+  struct EigLanes;                          // concurrent per-sector eigensolvers (tsc_dmrg.cu)
+  std::shared_ptr<EigLanes> eig;
   Lattice L;
   int tot_num_up = 0, tot_num_down = 0;
   SiteOp st_elec_up, st_elec_down, num_elec, st_sd, st_sz;
@@ -228,6 +239,8 @@ class Engine {
     double err, ent, ent_mult;
     int hpsi_calls;
     double hpsi_seconds, hpsi_flops, step_seconds;
+    // wall time of the step's parts (stream synchronised at each boundary)
+    double set_seconds, lanczos_seconds, truncate_seconds, grow_seconds, wave_seconds;
   };
   void run(int kept_min, int kept_warm, const std::vector<int>& sweeps, double lanzero_override,
            unsigned long long seed, std::vector<StepRec>* log, bool warmup_only = false);

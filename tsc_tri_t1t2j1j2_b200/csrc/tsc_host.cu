@@ -4,6 +4,10 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <map>
+#include <mutex>
+#include <unordered_map>
+#include <vector>
 
 #include "tsc_engine.hpp"
 
@@ -14,13 +18,143 @@ void cuda_check(cudaError_t e, const char* what) {
                                     std::string(what) + ": " + cudaGetErrorString(e));
 }
 
+// One stream-ordered pool per device that keeps freed memory for reuse (the
+// default pool hands it back to the driver at every synchronisation, so each
+// DMRG step would map its Krylov space and task buffers afresh).  Engines trim
+// it when they are destroyed.
+static std::mutex g_pool_mu;
+static cudaMemPool_t g_pools[256] = {};
+
+cudaMemPool_t device_pool() {
+  int dev = 0;
+  cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
+  if (dev < 0 || dev >= 256) throw Error(-1, "device ordinal out of range");
+  std::lock_guard<std::mutex> lock(g_pool_mu);
+  if (!g_pools[dev]) {
+    cudaMemPoolProps props = {};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    cudaMemPool_t pool = nullptr;
+    cuda_check(cudaMemPoolCreate(&pool, &props), "cudaMemPoolCreate");
+    uint64_t keep = UINT64_MAX;
+    cuda_check(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep), "cudaMemPoolSetAttribute");
+    g_pools[dev] = pool;
+  }
+  return g_pools[dev];
+}
+
+namespace {
+// Per-stream arena: chunks from the device pool, carved best fit, freed blocks
+// coalesced with their neighbours inside a chunk.  All blocks of one arena are
+// used in the order of its stream, so a block freed by the host can be handed
+// out again at once.
+struct Arena {
+  struct Chunk {
+    char* base;
+    size_t bytes;
+  };
+  std::vector<Chunk> chunks;
+  std::map<char*, size_t> free_at;             // block start -> bytes
+  std::multimap<size_t, char*> free_size;      // bytes -> block start
+  std::map<char*, char*> chunk_end;            // chunk base -> one past its end
+  size_t reserved = 0;
+
+  void insert_free(char* p, size_t n) {
+    free_at[p] = n;
+    free_size.emplace(n, p);
+  }
+  void erase_free(std::map<char*, size_t>::iterator it) {
+    auto r = free_size.equal_range(it->second);
+    for (auto q = r.first; q != r.second; ++q)
+      if (q->second == it->first) {
+        free_size.erase(q);
+        break;
+      }
+    free_at.erase(it);
+  }
+  char* chunk_limit(char* p) const {   // end of the chunk holding p
+    auto it = chunk_end.upper_bound(p);
+    --it;
+    return it->second;
+  }
+  char* take(size_t n) {
+    auto it = free_size.lower_bound(n);
+    if (it == free_size.end()) return nullptr;
+    char* p = it->second;
+    size_t have = it->first;
+    free_size.erase(it);
+    free_at.erase(p);
+    if (have > n) insert_free(p + n, have - n);
+    return p;
+  }
+  void give(char* p, size_t n) {
+    char* lim = chunk_limit(p);
+    auto nx = free_at.find(p + n);   // merge with the following free block
+    if (nx != free_at.end() && p + n < lim) {
+      n += nx->second;
+      erase_free(nx);
+    }
+    auto pv = free_at.lower_bound(p);   // and with the preceding one
+    if (pv != free_at.begin()) {
+      --pv;
+      if (pv->first + pv->second == p && chunk_limit(pv->first) == lim) {
+        p = pv->first;
+        n += pv->second;
+        erase_free(pv);
+      }
+    }
+    insert_free(p, n);
+  }
+};
+std::mutex g_arena_mu;
+std::unordered_map<cudaStream_t, Arena> g_arena;
+
+constexpr size_t kAlign = 256;
+constexpr size_t kMinChunk = 64ull << 20;
+constexpr size_t kMaxChunk = 4ull << 30;
+}  // namespace
+
+void release_stream_cache(cudaStream_t s) {
+  std::lock_guard<std::mutex> lock(g_arena_mu);
+  auto it = g_arena.find(s);
+  if (it == g_arena.end()) return;
+  for (auto& c : it->second.chunks) cudaFreeAsync(c.base, s);
+  g_arena.erase(it);
+}
+
 DevBuf::DevBuf(size_t count, cudaStream_t s, bool zero) : n(count), st(s) {
   if (count == 0) return;
-  cuda_check(cudaMallocAsync((void**)&p, count * sizeof(double2), s), "cudaMallocAsync");
+  cls = (count * sizeof(double2) + kAlign - 1) / kAlign * kAlign;
+  {
+    std::lock_guard<std::mutex> lock(g_arena_mu);
+    Arena& A = g_arena[s];
+    char* q = A.take(cls);
+    if (!q) {   // new chunk: geometric growth between 64 MiB and 4 GiB, at least the request
+      size_t want = std::max(cls, std::min(kMaxChunk, std::max(kMinChunk, A.reserved / 2)));
+      void* base = nullptr;
+      cudaError_t e = cudaMallocFromPoolAsync(&base, want, device_pool(), s);
+      if (e == cudaErrorMemoryAllocation && want > cls) {   // fall back to the exact request
+        cudaGetLastError();
+        want = cls;
+        e = cudaMallocFromPoolAsync(&base, want, device_pool(), s);
+      }
+      cuda_check(e, "cudaMallocFromPoolAsync");
+      A.chunks.push_back({static_cast<char*>(base), want});
+      A.chunk_end[static_cast<char*>(base)] = static_cast<char*>(base) + want;
+      A.reserved += want;
+      A.insert_free(static_cast<char*>(base), want);
+      q = A.take(cls);
+    }
+    p = reinterpret_cast<double2*>(q);
+  }
   if (zero) cuda_check(cudaMemsetAsync(p, 0, count * sizeof(double2), s), "cudaMemsetAsync");
 }
 DevBuf::~DevBuf() {
-  if (p) cudaFreeAsync(p, st);
+  if (!p) return;
+  std::lock_guard<std::mutex> lock(g_arena_mu);
+  auto it = g_arena.find(st);
+  if (it != g_arena.end()) it->second.give(reinterpret_cast<char*>(p), cls);
 }
 
 // ---- SU(2) coefficients --------------------------------------------------------
@@ -193,6 +327,7 @@ Engine::Engine(int Nx, int Ny, double t1, double t2, double J1, double J2, int d
   cuda_check(cudaGetDeviceCount(&ndev), "cudaGetDeviceCount");
   if (device < 0 || device >= ndev) throw Error(-1, "no such CUDA device");
   cuda_check(cudaSetDevice(device), "cudaSetDevice");
+  device_ = device;
   cuda_check(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "cudaStreamCreate");
   cuda_check(cudaEventCreate(&ev0), "cudaEventCreate");
   cuda_check(cudaEventCreate(&ev1), "cudaEventCreate");
@@ -227,10 +362,17 @@ Engine::~Engine() {
   env_truns.clear();
   disk_wave.reset();
   red_buf.reset();
+  eig.reset();
+  release_stream_cache(st);
   if (st) cudaStreamSynchronize(st);
+  try {
+    cudaMemPoolTrimTo(device_pool(), 0);
+  } catch (...) {
+  }
   if (h_scal) cudaFreeHost(h_scal);
   if (ev0) cudaEventDestroy(ev0);
   if (ev1) cudaEventDestroy(ev1);
+  for (cudaEvent_t e : hpsi_events) cudaEventDestroy(e);
   if (st) cudaStreamDestroy(st);
 }
 

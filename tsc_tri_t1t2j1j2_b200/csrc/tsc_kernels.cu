@@ -401,12 +401,19 @@ __device__ int sturm_count(const double* d, const double* e, int n, double x, do
   return c;
 }
 
-__global__ void tridiag_lowest_kernel(const double* __restrict__ d, const double* __restrict__ e, int n,
-                                      int want_vec, double* __restrict__ res, double* __restrict__ z) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+// Lowest eigenpair of the symmetric tridiagonal T (diag d[0..n), off-diagonal
+// e[0..n-1)), the part of dstev the Lanczos loop uses (eigen.f90:99-141).  One
+// warp: the eigenvalue by Sturm-count multisection (32 interior points per
+// round, each lane counting at one point, so a round shrinks the bracket 33x),
+// the eigenvector by inverse iteration in lane 0.  n <= 127.
+__device__ void tridiag_lowest_warp(const double* __restrict__ d, const double* __restrict__ e, int n,
+                                    int want_vec, double* __restrict__ res, double* __restrict__ z) {
+  const int lane = threadIdx.x & 31;
   if (n == 1) {
-    res[0] = d[0];
-    if (want_vec) z[0] = 1.0;
+    if (lane == 0) {
+      res[0] = d[0];
+      if (want_vec) z[0] = 1.0;
+    }
     return;
   }
   double lo = d[0], hi = d[0], emax = 0.0;
@@ -420,19 +427,32 @@ __global__ void tridiag_lowest_kernel(const double* __restrict__ d, const double
   const double pivmin = DBL_MIN * fmax(1.0, emax);
   lo -= 2.0 * DBL_EPSILON * tnorm + pivmin;
   hi += 2.0 * DBL_EPSILON * tnorm + pivmin;
-  // invariant: count(lo) == 0, count(hi) >= 1
-  for (int it = 0; it < 200; ++it) {
-    double mid = 0.5 * (lo + hi);
-    if (mid <= lo || mid >= hi) break;
+  // invariant: count(lo) == 0, count(hi) >= 1 (Gershgorin bounds)
+  for (int round = 0; round < 64; ++round) {
     if (hi - lo <= 2.0 * DBL_EPSILON * fmax(fabs(lo), fabs(hi)) + pivmin) break;
-    if (sturm_count(d, e, n, mid, pivmin) >= 1) hi = mid;
-    else lo = mid;
+    const double x = lo + (hi - lo) * (double)(lane + 1) * (1.0 / 33.0);
+    const bool above = (x < hi) && (x > lo) && sturm_count(d, e, n, x, pivmin) >= 1;
+    const unsigned ball = __ballot_sync(0xffffffffu, above);
+    const unsigned below = __ballot_sync(0xffffffffu, (x > lo) && (x < hi) && !above);
+    // new bracket: the lowest point with count >= 1, and the highest point
+    // under it with count 0 (points outside (lo, hi) by rounding are skipped)
+    const int j = ball ? __ffs(ball) - 1 : 32;
+    const unsigned under = below & (j >= 32 ? 0xffffffffu : ((1u << j) - 1u));
+    const int i = under ? 31 - __clz(under) : -1;
+    const double xj = __shfl_sync(0xffffffffu, x, j & 31);
+    const double xi = __shfl_sync(0xffffffffu, x, i < 0 ? 0 : i);
+    const double nhi = (j < 32) ? xj : hi;
+    const double nlo = (i >= 0) ? xi : lo;
+    if (nhi >= hi && nlo <= lo) break;   // no representable progress
+    lo = nlo;
+    hi = nhi;
   }
   const double lam = 0.5 * (lo + hi);
+  if (lane != 0) return;
   res[0] = lam;
   if (!want_vec) return;
   // inverse iteration on (T - lam I) with a partially pivoted tridiagonal LU
-  // (rows kept as diag/super1/super2 of U plus multipliers); n <= 101.
+  // (rows kept as diag/super1/super2 of U plus multipliers); n <= 127.
   double u0[128], u1[128], u2[128], lm[128], y[128];
   int piv[128];
   const double shift = lam;
@@ -492,6 +512,36 @@ __global__ void tridiag_lowest_kernel(const double* __restrict__ d, const double
     if (fabs(y[i]) > fabs(y[imax])) imax = i;
   const double sg = y[imax] < 0 ? -1.0 : 1.0;
   for (int i = 0; i < n; ++i) z[i] = sg * y[i];
+}
+
+
+__global__ void tridiag_lowest_kernel(const double* __restrict__ d, const double* __restrict__ e, int n,
+                                      int want_vec, double* __restrict__ res, double* __restrict__ z) {
+  tridiag_lowest_warp(d, e, n, want_vec, res, z);
+}
+
+// End of one Lanczos iteration, on the device: beta[k-1] = sqrt(n2), the
+// lowest Ritz value of T_k (alpha[1..k], beta[1..k-1]), and a packet
+// {ritz, n2, alpha[k]} for a single read-back by the host.
+__global__ void lanczos_tail_kernel(const double* __restrict__ n2, double* __restrict__ alpha,
+                                    double* __restrict__ beta, int k, double* __restrict__ res,
+                                    double* __restrict__ packet) {
+  __shared__ double sd[128], se[128];
+  const int lane = threadIdx.x & 31;
+  const double b = sqrt(n2[0]);
+  for (int i = lane; i < k; i += 32) {
+    sd[i] = alpha[i + 1];
+    se[i] = (i + 1 < k - 1) ? beta[i + 1] : (i + 1 == k - 1 ? b : 0.0);
+  }
+  __syncwarp();
+  if (lane == 0) beta[k - 1] = b;
+  tridiag_lowest_warp(sd, se, k, 0, res, nullptr);
+  __syncwarp();
+  if (lane == 0) {
+    packet[0] = res[0];
+    packet[1] = n2[0];
+    packet[2] = alpha[k];
+  }
 }
 
 __global__ void phase_fix_kernel(double2* __restrict__ U, int rows) {
@@ -614,8 +664,15 @@ cudaError_t launch_phase_fix(double2* U, int rows, int cols, cudaStream_t st) {
 
 cudaError_t launch_tridiag_lowest(const double* d, const double* e, int n, int want_vec, double* res, double* z,
                                   cudaStream_t st) {
-  if (n > 128) return cudaErrorInvalidValue;
+  if (n < 1 || n > 127) return cudaErrorInvalidValue;
   tridiag_lowest_kernel<<<1, 32, 0, st>>>(d, e, n, want_vec, res, z);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_lanczos_tail(const double* n2, double* alpha, double* beta, int k, double* res, double* packet,
+                                cudaStream_t st) {
+  if (k < 1 || k > 127) return cudaErrorInvalidValue;
+  lanczos_tail_kernel<<<1, 32, 0, st>>>(n2, alpha, beta, k, res, packet);
   return cudaGetLastError();
 }
 

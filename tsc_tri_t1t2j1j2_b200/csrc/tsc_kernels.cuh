@@ -83,5 +83,9 @@ cudaError_t launch_phase_fix(double2* U, int rows, int cols, cudaStream_t st);
 // res[0]=E0 and, if want_vec, z[0..n) the normalised eigenvector.
 cudaError_t launch_tridiag_lowest(const double* d, const double* e, int n, int want_vec, double* res,
                                   double* z, cudaStream_t st);
+// beta[k-1] = sqrt(*n2); res[0] = lowest eigenvalue of T_k (alpha[1..k], beta[1..k-1],
+// 1-based slots); packet = {res[0], *n2, alpha[k]}.  k <= 127.
+cudaError_t launch_lanczos_tail(const double* n2, double* alpha, double* beta, int k, double* res, double* packet,
+                                cudaStream_t st);
 
 }  // namespace tsc
