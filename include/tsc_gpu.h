@@ -72,6 +72,10 @@ typedef struct tsc_step_log {
    * Lanczos (H.psi included), density matrix + truncation, block growth +
    * renormalisation, wave transformation */
   double set_seconds, lanczos_seconds, truncate_seconds, grow_seconds, wave_seconds;
+  /* split-precision form only (else 0): iterations on the BF16-sliced H.psi
+   * and their last Ritz value, before the FP64 iterations that finish the solve */
+  int split_iters;
+  double split_e0;
 } tsc_step_log;
 
 typedef struct tsc_ctx tsc_ctx;
@@ -153,6 +157,22 @@ int tsc_hpsi_stats(tsc_ctx* ctx, double* device_ms, double* ref_flops, double* e
 /* The context's CUDA stream (cudaStream_t as void*): device-pointer calls are
  * enqueued on it, so callers can order their own work and time it with events. */
 void* tsc_stream(tsc_ctx* ctx);
+
+/* Arithmetic of the H.psi sector GEMMs (the reference computes everything in
+ * complex FP64 and has no such switch).  TSC_FP64: complex FP64 throughout.
+ * TSC_SPLIT_BF16: every FP64 operand split into three BF16 slices multiplied
+ * on the tensor cores with FP32 accumulation (about 1e-6 relative error per
+ * H.psi); Lanczos iterates on that H.psi until successive Ritz values agree to
+ * split_tol relative (<= 0 keeps the current value, 1e-9 at creation), then
+ * runs the reference's FP64 iterations from that vector until the FP64
+ * residual ||H psi - E psi|| is below 0.1 sqrt(lanzero), so the energy and
+ * vector it returns are FP64 results.  Orthogonalisation, tridiagonal solve,
+ * density-matrix eigensolver, renormalisation and wave transforms stay FP64,
+ * and so do the warm-up steps of tsc_dmrg_run.  Takes effect from the next
+ * superblock set. */
+#define TSC_FP64 0
+#define TSC_SPLIT_BF16 1
+int tsc_set_precision(tsc_ctx* ctx, int mode, double split_tol);
 
 /* H.psi on device pointers that allocates nothing (no counterpart in the
  * reference).  For callers that cannot call cudaMalloc or any allocating

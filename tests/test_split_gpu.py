@@ -1,0 +1,94 @@
+"""Split-precision form (BF16 slices on tcgen05, FP32 accumulation, Lanczos
+finished in FP64) against the FP64 engine and the oracle, through the C-ABI.
+
+Tolerances: split H.psi max|dx|/max|x| <= 2e-5 against the FP64 H.psi (three
+BF16 slices with FP32 accumulation: ~1e-6 on physical superblocks, ~1.6e-5 on
+the random-valued YC4x12 m=1000 superblock); ground-state energy after the FP64
+refinement |dE/E| <= 1e-10 against the oracle, for single solves and for the
+last quarter of the steps of a full small run at lanzero = 1e-13.
+"""
+import numpy as np
+import pytest
+
+import orc
+from _capture import parse_oracle_capture
+from tsc_tri_t1t2j1j2_b200 import Context
+
+SPLIT = Context.SPLIT_BF16
+
+
+def rel(a, b):
+    return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
+
+
+@pytest.fixture(scope="module", params=[(4, 0.3, 0.036, 60, 6), (4, 0.3, 0.036, 120, 9), (4, 0.0, 0.0, 80, 22)],
+                ids=lambda c: f"Nx{c[0]}_t2{c[1]}_m{c[3]}_s{c[4]}")
+def captured(request):
+    Nx, t2, J2, kept, step = request.param
+    cfg = orc.RunConfig(Nx=Nx, Ny=4, t1=1.0, t2=t2, J1=0.4, J2=J2, kept_min=kept, kept_warm=kept,
+                        sweeps=[kept], lanzero=1e-10)
+    o = orc.Oracle(cfg, capture_step=step)
+    o.run()
+    cap = parse_oracle_capture(*o.capture())
+    ctx = Context(Nx, 4, 1.0, t2, 0.4, J2)
+    ctx.set_precision(SPLIT)
+    ctx.set_superblock(cap["sys"], cap["env"], cap["sys_bs"], cap["env_bs"], cap["psi0"])
+    yield cap, ctx
+    ctx.close()
+
+
+@pytest.mark.gpu
+def test_split_hpsi_close_to_fp64(captured):
+    cap, ctx = captured
+    out = ctx.model_wave(cap["psi0"].vec)
+    assert rel(out, cap["hpsi"].vec) <= 2e-5
+
+
+@pytest.mark.gpu
+def test_split_lanczos_energy(captured):
+    cap, ctx = captured
+    vec, e0, iters = ctx.lanczos_memo_new(cap["psi0"].vec, 1e-10)
+    assert abs(e0 - cap["e0"]) <= 1e-10 * abs(cap["e0"])
+    assert abs(abs(np.vdot(vec, cap["gs"].vec)) - 1.0) <= 1e-8
+
+
+@pytest.mark.gpu
+def test_split_hpsi_bench_superblock():
+    import bench
+    sl, el, ints, data, off, n = bench.make_superblock()
+    outs = []
+    for mode in (Context.FP64, SPLIT):
+        ctx = Context(**bench.MODEL)
+        try:
+            ctx.set_precision(mode)
+            ctx.set_superblock_flat(sl, el, ints, data)
+            outs.append(ctx.model_wave(data[off:off + n]))
+        finally:
+            ctx.close()
+    assert rel(outs[1], outs[0]) <= 2e-5
+
+
+@pytest.mark.gpu
+def test_split_full_run_energies():
+    """A whole run in the split form against the oracle's.  The reference stops
+    Lanczos when successive Ritz values agree to lanzero, which leaves its
+    vectors about sqrt(lanzero/gap) from the eigenvector; a different (correct)
+    solver then truncates a slightly different basis and the two runs drift
+    apart by ~1e-9 at lanzero = 1e-10.  With lanzero = 1e-13 both runs are
+    converged well below that and the last quarter of the steps agree to
+    better than 1e-10 relative (about 4e-11 measured)."""
+    cfg = orc.RunConfig(Nx=3, Ny=4, t1=1.0, t2=0.3, J1=0.4, J2=0.036, kept_min=40, kept_warm=40, sweeps=[40],
+                        lanzero=1e-13)
+    ref_steps = orc.Oracle(cfg).run()
+    ctx = Context(3, 4, 1.0, 0.3, 0.4, 0.036)
+    try:
+        ctx.set_precision(SPLIT, 1e-11)
+        steps = ctx.get_ground_state(kept_min=40, kept_warm=40, sweeps=[40], lanzero=1e-13)
+    finally:
+        ctx.close()
+    assert len(steps) == len(ref_steps)
+    assert sum(s["split_iters"] for s in steps) > 0
+    tail = len(steps) // 4
+    e = np.array([s["e0"] for s in steps])[-tail:]
+    er = np.array([s["e0"] for s in ref_steps])[-tail:]
+    assert np.max(np.abs(e - er) / np.abs(er)) <= 1e-10

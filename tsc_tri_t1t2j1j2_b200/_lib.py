@@ -19,7 +19,7 @@ EXPORTED = [
     "tsc_create", "tsc_destroy", "tsc_last_error", "tsc_tot_num_up", "tsc_superblock_set",
     "tsc_superblock_dim", "tsc_hpsi", "tsc_hpsi_device", "tsc_lanczos", "tsc_truncate",
     "tsc_renormalize", "tsc_wave_transform", "tsc_dmrg_run", "tsc_set_capture", "tsc_get_capture",
-    "tsc_hpsi_stats", "tsc_stream", "tsc_hpsi_noalloc",
+    "tsc_hpsi_stats", "tsc_stream", "tsc_hpsi_noalloc", "tsc_set_precision",
 ]
 
 
@@ -40,7 +40,7 @@ class StepLog(ctypes.Structure):
                 ("entropy_mult", c_double), ("hpsi_calls", c_int), ("hpsi_seconds", c_double),
                 ("hpsi_flops", c_double), ("step_seconds", c_double), ("set_seconds", c_double),
                 ("lanczos_seconds", c_double), ("truncate_seconds", c_double), ("grow_seconds", c_double),
-                ("wave_seconds", c_double)]
+                ("wave_seconds", c_double), ("split_iters", c_int), ("split_e0", c_double)]
 
 
 class TscError(RuntimeError):
@@ -84,6 +84,7 @@ def load():
     L.tsc_stream.argtypes = [c_void]
     L.tsc_stream.restype = c_void
     L.tsc_hpsi_noalloc.argtypes = [c_void, c_void, c_void]
+    L.tsc_set_precision.argtypes = [c_void, c_int, c_double]
     _lib = L
     return L
 

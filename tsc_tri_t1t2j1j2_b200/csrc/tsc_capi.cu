@@ -351,7 +351,7 @@ int tsc_dmrg_run(tsc_ctx* ctx, const tsc_sweep_config* sw, tsc_step_log* log, in
       log[i] = tsc_step_log{s.phase, s.sys_len, s.env_len, s.e0, s.iters, s.num_state, s.err, s.ent, s.ent_mult,
                             s.hpsi_calls, s.hpsi_seconds, s.hpsi_flops, s.step_seconds,
                             s.set_seconds, s.lanczos_seconds, s.truncate_seconds, s.grow_seconds,
-                            s.wave_seconds};
+                            s.wave_seconds, s.split_iters, s.split_e0};
     }
   });
   return rc == TSC_OK ? nsteps : rc;
@@ -381,3 +381,12 @@ int tsc_get_capture(tsc_ctx* ctx, const int** ints, long long* nints, const doub
 }
 
 }  // extern "C"
+
+int tsc_set_precision(tsc_ctx* ctx, int mode, double split_tol) {
+  return guard(ctx, [&] {
+    if (!ctx->eng) throw Error(TSC_E_STATE, "no engine");
+    if (mode != TSC_FP64 && mode != TSC_SPLIT_BF16) throw Error(TSC_E_ARG, "unknown precision mode");
+    ctx->eng->precision_ = mode;
+    if (split_tol > 0) ctx->eng->split_tol_ = split_tol;
+  });
+}

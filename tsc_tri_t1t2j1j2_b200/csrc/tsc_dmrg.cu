@@ -124,7 +124,7 @@ inline double pm1(int e) { return ((e % 2) + 2) % 2 == 0 ? 1.0 : -1.0; }
 inline long long absoff(const double2* p) { return (long long)((uintptr_t)p / sizeof(double2)); }
 
 // scalar slots in d_scal
-constexpr int S_ALPHA = 0, S_BETA = 128, S_UV = 256, S_UU = 384, S_RES = 512, S_Z = 520, S_N2 = 700, S_PKT = 704;
+constexpr int S_ALPHA = 0, S_BETA = 128, S_UV = 256, S_UU = 384, S_RES = 512, S_Z = 520, S_N2 = 700, S_PKT = 704, S_CHK = 712, S_ZR = 768;
 
 // Density-matrix eigenvalues below this are rounding noise (rho has unit trace).
 constexpr double kZeroWeight = 1e-13;
@@ -187,6 +187,36 @@ void quicksort_double(std::vector<double>& a, std::vector<int>& idx, int lo, int
 
 // ---------------------------------------------------------------------------- Lanczos
 void Engine::lanczos(double2* d_psi, double lanzero, int* iters, double* e0, double* hpsi_ms, int* hpsi_calls) {
+  last_split_iters = 0;
+  last_split_e0 = 0.0;
+  if (!sb.p1s.split) {
+    lanczos_run(d_psi, lanzero, 0.0, false, iters, e0, hpsi_ms, hpsi_calls);
+    return;
+  }
+  // Split-precision form: Lanczos on the BF16-sliced H.psi until the Ritz value
+  // settles to split_tol relative (the slices' noise floor), then FP64 Lanczos
+  // from that vector until the residual of its Ritz pair is below
+  // 0.1 sqrt(lanzero), which bounds the energy error by about 0.01 lanzero/gap.
+  // (Stopping on successive Ritz values, as the reference does, is premature
+  // from a start this close to the eigenvector.)
+  int it1 = 0, it2 = 0, c1 = 0, c2 = 0;
+  double ms1 = 0.0, ms2 = 0.0, e_split = 0.0;
+  lanczos_run(d_psi, lanzero, split_tol_, true, &it1, &e_split, &ms1, &c1);
+  int fault = 0;
+  cuda_check(split_fault_flag(&fault, 1), "split fault flag");
+  if (fault) throw Error(-3, "split-precision kernel: a bounded wait ran out");
+  // FP64 Lanczos from that vector, stopped on the Ritz residual
+  // ||H psi - E psi|| <= 0.1 sqrt(lanzero) (from the tridiagonal, no extra H.psi)
+  lanczos_run(d_psi, lanzero, 0.0, false, &it2, e0, &ms2, &c2, 0.1 * std::sqrt(lanzero));
+  last_split_iters = it1;
+  last_split_e0 = e_split;
+  *iters = it1 + it2;
+  if (hpsi_ms) *hpsi_ms = ms1 + ms2;
+  if (hpsi_calls) *hpsi_calls = c1 + c2;
+}
+
+void Engine::lanczos_run(double2* d_psi, double lanzero, double rel_tol, bool split, int* iters, double* e0,
+                         double* hpsi_ms, int* hpsi_calls, double res_tol) {
   if (!sb.valid) throw Error(-4, "no superblock");
   const long long n = sb.wl.dim;
   const int loop_in = 100, loop_out = 4;
@@ -213,7 +243,7 @@ void Engine::lanczos(double2* d_psi, double lanzero, int* iters, double* e0, dou
       }
     }
     cuda_check(cudaEventRecord(hpsi_events[2 * calls], st), "event");
-    hpsi(v(j), v(j + 1));
+    hpsi_form(v(j), v(j + 1), split);
     cuda_check(cudaEventRecord(hpsi_events[2 * calls + 1], st), "event");
     calls++;
   };
@@ -239,6 +269,7 @@ void Engine::lanczos(double2* d_psi, double lanzero, int* iters, double* e0, dou
     cuda_check(launch_multi_dot(v(1), ld, 1, v(2), n, d_part, a_d + 1, st), "alpha");
     read_back(S_ALPHA + 1, 1);
     ritzmin = h_scal[S_ALPHA + 1];
+    double zlast = 1.0;   // T_1 = [alpha_1]: its eigenvector is (1)
     bool conv = false;
     while (last < loop_in) {
       // One iteration runs on the device without a host decision; the host
@@ -260,16 +291,25 @@ void Engine::lanczos(double2* d_psi, double lanzero, int* iters, double* e0, dou
       cuda_check(launch_multi_dot(w, ld, 1, w, n, d_part, uu_d + last + 1, st), "uu");
       do_hpsi(last + 1);
       cuda_check(launch_multi_dot(v(last + 1), ld, 1, v(last + 2), n, d_part, a_d + last + 1, st), "alpha");
-      cuda_check(launch_lanczos_tail(d_scal + S_N2, a_d, b_d, last + 1, d_scal + S_RES, d_scal + S_PKT, st), "tail");
-      read_back(S_PKT, 3);
+      cuda_check(launch_lanczos_tail(d_scal + S_N2, a_d, b_d, last + 1, d_scal + S_RES, d_scal + S_PKT,
+                                     res_tol > 0 ? d_scal + S_ZR : nullptr, st),
+                 "tail");
+      read_back(S_PKT, 4);
       const double beta_last = std::sqrt(h_scal[S_PKT + 1]);
       if (std::fabs(beta_last) <= lanzero) {
         conv = true;
         break;
       }
+      // residual stop: ||H y - theta y|| = beta_last |z_last| for the Ritz pair of T_last
+      if (res_tol > 0 && beta_last * zlast <= res_tol) {
+        conv = true;
+        break;
+      }
+      zlast = h_scal[S_PKT + 3];
       last++;
       const double d0 = h_scal[S_PKT];
-      if (std::fabs(d0 - ritzmin) <= lanzero || (last == loop_in && iter_out == loop_out)) {
+      const double tol = std::max(lanzero, rel_tol * std::fabs(d0));
+      if ((res_tol <= 0 && std::fabs(d0 - ritzmin) <= tol) || (last == loop_in && iter_out == loop_out)) {
         ritzmin = d0;
         lastmin = ritzmin;
         conv = true;
@@ -1227,6 +1267,8 @@ void Engine::lanczos_step(int phase, DModel& sys, DModel& env, const Basis& sys_
   t1 = phase_clock(st);
   lanczos(psi->p, lanzero_, &rec.iters, &rec.e0, &hms, &calls);
   rec.lanczos_seconds = secs(t1, phase_clock(st));
+  rec.split_iters = last_split_iters;
+  rec.split_e0 = last_split_e0;
   rec.hpsi_calls = calls;
   rec.hpsi_seconds = hms * 1e-3;
   rec.hpsi_flops = sb.ref_flops * calls;
@@ -1234,6 +1276,11 @@ void Engine::lanczos_step(int phase, DModel& sys, DModel& env, const Basis& sys_
 }
 
 void Engine::warm_up(int end_id, double trun_err, std::vector<StepRec>* log) {
+  struct Flag {
+    bool& f;
+    explicit Flag(bool& x) : f(x) { f = true; }
+    ~Flag() { f = false; }
+  } in_warmup(in_warmup_);
   int label = 1;
   L.setup(1, 1);
   DModel sys = site_model(), env = site_model();

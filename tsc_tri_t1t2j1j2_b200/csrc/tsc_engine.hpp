@@ -153,6 +153,7 @@ struct TaskList {
   GReduce* d_reds = nullptr;
   int njobs = 0, nreds = 0;
   int tile = 64;           // CTA tile edge used for this list (64 or 32)
+  bool split = false;      // jobs are 128 x 64 tiles for the split-precision kernel
   long long max_red_elems = 0;
   DevBufP part;            // partial tiles of split groups
   long long part_elems = 0;
@@ -163,6 +164,8 @@ struct TaskList {
   // total_cost / (slots * waves) are split into contiguous term chunks, each
   // computing a partial tile; a fixed-order reduction then writes the group.
   void upload(cudaStream_t st, int slots = 296, int waves = 4);
+  // The same lists for the split-precision kernel (the host lists are kept).
+  void upload_split(cudaStream_t st);
 };
 
 struct Stats {
@@ -195,6 +198,7 @@ class Engine {
     std::vector<OpSet> sub_s_sys, sub_s_env;   // merged block-block operators
     TaskList merge;            // hmerge axpy tasks
     TaskList p1, p2;           // H.psi phase 1 (intermediates) and phase 2 (outputs)
+    TaskList p1s, p2s;         // the same, tiled for the split-precision kernel
     long long scratch_elems = 0;
     DevBufP scratch;
     double ref_flops = 0;      // algorithmic flops of one model_wave (reference order)
@@ -202,11 +206,23 @@ class Engine {
   } sb;
 
   void superblock_set(DModel&& sys, DModel&& env, Basis&& sys_bs, Basis&& env_bs, WLayout&& wl);
-  void hpsi(const double2* d_in, double2* d_out);   // enqueue on st
+  void hpsi(const double2* d_in, double2* d_out);   // enqueue on st, in the context's precision
+  void hpsi_form(const double2* d_in, double2* d_out, bool split);
+  // 0: complex FP64 throughout; 1: H.psi sector GEMMs as BF16 slices on the
+  // tensor cores, Lanczos finished by FP64 iterations.  Applies from the next
+  // superblock set on.
+  int precision_ = 0;
+  double split_tol_ = 1e-9;   // relative Ritz-value change that ends the split iterations
+  bool split_now_ = false;    // the current superblock's solve uses the split form
+  bool in_warmup_ = false;    // set while the warm-up (infinite-lattice) steps run
   Stats last_stats;
 
   // Lanczos (eigen.f90:4-199) on the current superblock; psi device buffer in/out
   void lanczos(double2* d_psi, double lanzero, int* iters, double* e0, double* hpsi_ms, int* hpsi_calls);
+  void lanczos_run(double2* d_psi, double lanzero, double rel_tol, bool split, int* iters, double* e0,
+                   double* hpsi_ms, int* hpsi_calls, double res_tol = 0.0);
+  int last_split_iters = 0;     // split-precision iterations of the last solve
+  double last_split_e0 = 0.0;   // their final Ritz value
 
   // density matrix + truncation (den_mat.f90)
   struct TruncResult {
@@ -241,6 +257,8 @@ class Engine {
     double hpsi_seconds, hpsi_flops, step_seconds;
     // wall time of the step's parts (stream synchronised at each boundary)
     double set_seconds, lanczos_seconds, truncate_seconds, grow_seconds, wave_seconds;
+    int split_iters;
+    double split_e0;
   };
   void run(int kept_min, int kept_warm, const std::vector<int>& sweeps, double lanzero_override,
            unsigned long long seed, std::vector<StepRec>* log, bool warmup_only = false);

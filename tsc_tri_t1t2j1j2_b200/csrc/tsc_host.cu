@@ -499,10 +499,20 @@ int default_tile() {
   return t;
 }
 
+void TaskList::upload_split(cudaStream_t st) {
+  split = true;
+  upload(st, 148 * 2, 4);
+}
+
 void TaskList::upload(cudaStream_t st, int slots, int waves) {
   tile = default_tile();
-  const int TMt = tile, TNt = tile;
-  if (tile == 32) slots *= 3;
+  int TMt = tile, TNt = tile;
+  if (split) {
+    TMt = SPLIT_TILE_M;
+    TNt = SPLIT_TILE_N;
+  } else if (tile == 32) {
+    slots *= 3;
+  }
   std::vector<GTerm> terms;
   struct JC {
     GJob j;
@@ -594,8 +604,6 @@ void TaskList::upload(cudaStream_t st, int slots, int waves) {
   cuda_check(cudaMemcpyAsync(base, host.data(), total_b, cudaMemcpyHostToDevice, st), "task upload");
   part = part_elems ? std::make_shared<DevBuf>((size_t)part_elems, st, false) : nullptr;
   cuda_check(cudaStreamSynchronize(st), "task upload sync");
-  gterms.clear();
-  gterms.shrink_to_fit();
 }
 
 void Engine::run_tasks(TaskList& tl, double2* in, double2* out, double2* scr) {
@@ -605,7 +613,10 @@ void Engine::run_tasks(TaskList& tl, double2* in, double2* out, double2* scr) {
   b.p[2] = out;
   b.p[3] = scr;
   b.part = tl.part ? tl.part->p : nullptr;
-  cuda_check(launch_grouped_zgemm(tl.d_jobs, tl.njobs, tl.d_groups, tl.d_terms, b, st, tl.tile), "grouped_zgemm");
+  if (tl.split)
+    cuda_check(launch_grouped_zgemm_split(tl.d_jobs, tl.njobs, tl.d_groups, tl.d_terms, b, st), "grouped_zgemm_split");
+  else
+    cuda_check(launch_grouped_zgemm(tl.d_jobs, tl.njobs, tl.d_groups, tl.d_terms, b, st, tl.tile), "grouped_zgemm");
   if (tl.nreds)
     cuda_check(launch_reduce_partials(tl.d_reds, tl.nreds, tl.d_groups, b, tl.max_red_elems, st), "reduce_partials");
 }

@@ -972,8 +972,20 @@ void Engine::build_hpsi_tasks() {
   }
   S.ref_flops = B.ref_flops;
   S.scratch_elems = B.scr;
+  if (split_now_) {
+    S.p1s.groups = S.p1.groups;
+    S.p1s.gterms = S.p1.gterms;
+    S.p2s.groups = S.p2.groups;
+    S.p2s.gterms = S.p2.gterms;
+    S.p1s.upload_split(st);
+    S.p2s.upload_split(st);
+    S.p1s.gterms.clear();
+    S.p2s.gterms.clear();
+  }
   S.p1.upload(st);
   S.p2.upload(st);
+  S.p1.gterms.clear();
+  S.p2.gterms.clear();
   S.scratch = std::make_shared<DevBuf>((size_t)std::max<long long>(B.scr, 1), st, false);
 }
 
@@ -985,19 +997,27 @@ void Engine::superblock_set(DModel&& sys, DModel&& env, Basis&& sys_bs, Basis&& 
   sb.env_bs = std::move(env_bs);
   sb.wl = std::move(wl);
   L.setup(sb.sys.len, sb.env.len);
+  // warm-up steps stop Lanczos at a loose tolerance, where the reference's
+  // iteration path decides the result: they stay FP64 in either precision
+  split_now_ = precision_ == 1 && !in_warmup_;
   build_merge();
   build_hpsi_tasks();
   cuda_check(cudaStreamSynchronize(st), "superblock sync");
   sb.valid = true;
 }
 
-void Engine::hpsi(const double2* d_in, double2* d_out) {
+void Engine::hpsi(const double2* d_in, double2* d_out) { hpsi_form(d_in, d_out, sb.p1s.split); }
+
+void Engine::hpsi_form(const double2* d_in, double2* d_out, bool split) {
   if (!sb.valid) throw Error(-4, "no superblock");
+  TaskList& a = split ? sb.p1s : sb.p1;
+  TaskList& b = split ? sb.p2s : sb.p2;
+  if (split && !a.split) throw Error(-4, "split-precision lists were not built for this superblock");
   cuda_check(cudaEventRecord(ev0, st), "event");
-  run_tasks(sb.p1, const_cast<double2*>(d_in), d_out, sb.scratch->p);
-  run_tasks(sb.p2, const_cast<double2*>(d_in), d_out, sb.scratch->p);
+  run_tasks(a, const_cast<double2*>(d_in), d_out, sb.scratch->p);
+  run_tasks(b, const_cast<double2*>(d_in), d_out, sb.scratch->p);
   cuda_check(cudaEventRecord(ev1, st), "event");
-  last_stats.launches = (sb.p1.njobs > 0) + (sb.p2.njobs > 0) + (sb.p1.nreds > 0) + (sb.p2.nreds > 0);
+  last_stats.launches = (a.njobs > 0) + (b.njobs > 0) + (a.nreds > 0) + (b.nreds > 0);
   last_stats.hpsi_flops = sb.ref_flops;
 }
 

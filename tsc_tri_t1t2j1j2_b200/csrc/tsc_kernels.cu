@@ -525,7 +525,7 @@ __global__ void tridiag_lowest_kernel(const double* __restrict__ d, const double
 // {ritz, n2, alpha[k]} for a single read-back by the host.
 __global__ void lanczos_tail_kernel(const double* __restrict__ n2, double* __restrict__ alpha,
                                     double* __restrict__ beta, int k, double* __restrict__ res,
-                                    double* __restrict__ packet) {
+                                    double* __restrict__ packet, double* __restrict__ zbuf) {
   __shared__ double sd[128], se[128];
   const int lane = threadIdx.x & 31;
   const double b = sqrt(n2[0]);
@@ -535,12 +535,13 @@ __global__ void lanczos_tail_kernel(const double* __restrict__ n2, double* __res
   }
   __syncwarp();
   if (lane == 0) beta[k - 1] = b;
-  tridiag_lowest_warp(sd, se, k, 0, res, nullptr);
+  tridiag_lowest_warp(sd, se, k, zbuf ? 1 : 0, res, zbuf);
   __syncwarp();
   if (lane == 0) {
     packet[0] = res[0];
     packet[1] = n2[0];
     packet[2] = alpha[k];
+    packet[3] = zbuf ? fabs(zbuf[k - 1]) : 0.0;   // last component of the Ritz vector of T_k
   }
 }
 
@@ -670,9 +671,9 @@ cudaError_t launch_tridiag_lowest(const double* d, const double* e, int n, int w
 }
 
 cudaError_t launch_lanczos_tail(const double* n2, double* alpha, double* beta, int k, double* res, double* packet,
-                                cudaStream_t st) {
+                                double* zbuf, cudaStream_t st) {
   if (k < 1 || k > 127) return cudaErrorInvalidValue;
-  lanczos_tail_kernel<<<1, 32, 0, st>>>(n2, alpha, beta, k, res, packet);
+  lanczos_tail_kernel<<<1, 32, 0, st>>>(n2, alpha, beta, k, res, packet, zbuf);
   return cudaGetLastError();
 }
 

@@ -59,6 +59,14 @@ constexpr int GEMM_TK = 16, GEMM_THREADS = 128;
 // tile = CTA output tile edge (64: 64x64, 2 CTAs/SM; 32: 32x32, 6 CTAs/SM)
 cudaError_t launch_grouped_zgemm(const GJob* jobs, int njobs, const GGroup* groups, const GTerm* terms,
                                  Bases bases, cudaStream_t st, int tile);
+// Split-precision form of launch_grouped_zgemm (BF16 slices on tcgen05, FP32
+// accumulation in tensor memory); jobs are 128 x 64 tiles of the same groups.
+cudaError_t launch_grouped_zgemm_split(const GJob* jobs, int njobs, const GGroup* groups, const GTerm* terms,
+                                       Bases bases, cudaStream_t st);
+// Reads (and optionally clears) the flag the split kernel sets when one of its
+// bounded mbarrier waits runs out.
+cudaError_t split_fault_flag(int* host_flag, int clear);
+constexpr int SPLIT_TILE_M = 128, SPLIT_TILE_N = 64;
 cudaError_t launch_reduce_partials(const GReduce* reds, int nred, const GGroup* groups, Bases bases,
                                    long long max_elems, cudaStream_t st);
 
@@ -84,8 +92,9 @@ cudaError_t launch_phase_fix(double2* U, int rows, int cols, cudaStream_t st);
 cudaError_t launch_tridiag_lowest(const double* d, const double* e, int n, int want_vec, double* res,
                                   double* z, cudaStream_t st);
 // beta[k-1] = sqrt(*n2); res[0] = lowest eigenvalue of T_k (alpha[1..k], beta[1..k-1],
-// 1-based slots); packet = {res[0], *n2, alpha[k]}.  k <= 127.
+// 1-based slots); packet = {res[0], *n2, alpha[k], |z[k-1]|} where z (written to
+// zbuf when it is not null, else 0) is that eigenvalue's unit eigenvector.  k <= 127.
 cudaError_t launch_lanczos_tail(const double* n2, double* alpha, double* beta, int k, double* res, double* packet,
-                                cudaStream_t st);
+                                double* zbuf, cudaStream_t st);
 
 }  // namespace tsc

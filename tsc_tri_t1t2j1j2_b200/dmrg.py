@@ -103,6 +103,14 @@ class Context:
         """H.psi on device pointers (e.g. torch tensors' data_ptr()), enqueued on the context stream."""
         self._check(self.L.tsc_hpsi_device(self.h, ctypes.c_void_p(d_in), ctypes.c_void_p(d_out)))
 
+    FP64, SPLIT_BF16 = 0, 1
+
+    def set_precision(self, mode: int, split_tol: float = 0.0):
+        """H.psi arithmetic: Context.FP64 (default) or Context.SPLIT_BF16 (BF16 slices
+        on the tensor cores, Lanczos finished in FP64).  Applies from the next
+        superblock set."""
+        self._check(self.L.tsc_set_precision(self.h, int(mode), float(split_tol)))
+
     def hpsi_noalloc(self, d_in: int, d_out: int):
         """H.psi on device pointers that allocates nothing (scratch: a fixed 64 MiB
         device array shared by all calls; see include/tsc_gpu.h)."""
