@@ -12,14 +12,20 @@
 // so the result carries about 1e-6 relative error against the FP64 product.
 // Element terms and the write-back (beta, partial tiles) are done in FP64.
 //
-// CTA = one job: a 128 x 64 output tile of one group over a term range.  256
-// threads convert the FP64 operands of one K=16 step into the 12 BF16 planes
-// (3 slices x re/im, for A and B) of a shared-memory stage in the canonical
-// K-major, no-swizzle UMMA layout; one thread issues the step's 24 MMAs and
-// commits them to the stage's mbarrier, which frees the stage for the
-// conversion three steps later.  Every mbarrier wait is bounded: on timeout
-// the kernel records the fact in a device flag, waits (bounded) for its own
-// MMAs, frees its tensor memory and returns.
+// Persistent and warp-specialised: one CTA per SM walks the jobs blockIdx.x,
+// +gridDim.x, ... (128 x 64 output tiles of a group over a term range, in
+// longest-first order).  12 producer warps convert the FP64 operands of one
+// K=16 step -- one 8-element chunk per thread, the next step's loads in flight
+// while the current one converts -- into the 12 BF16 planes (3 slices x re/im,
+// for A and B) of a shared-memory stage in the canonical K-major, no-swizzle
+// UMMA layout, and arrive on the stage's full barrier; one lane of the MMA warp
+// issues the step's 24 MMAs into one of two TMEM accumulators and commits them
+// to the stage's empty barrier (and, after a job's last step, to the
+// accumulator's full barrier); 4 epilogue warps drain the other accumulator,
+// add the FP64 element terms and write the tile while the next job runs.
+// Every mbarrier wait is bounded: on timeout the kernel raises a CTA abort flag
+// and a device fault flag, waits (bounded) for its own MMAs, frees its tensor
+// memory and returns.
 #include <cuda_bf16.h>
 #include <cstdint>
 
@@ -31,12 +37,14 @@ __device__ int g_split_fault = 0;
 
 namespace {
 
-constexpr int SP_TM = 128, SP_TN = 64, SP_TK = 16, SP_STAGES = 3, SP_THREADS = 256;
+constexpr int SP_TM = 128, SP_TN = 64, SP_TK = 16, SP_STAGES = 4;
+constexpr int SP_PRODUCER_WARPS = 12, SP_MMA_WARP = 12, SP_EPI_WARP0 = 13;
+constexpr int SP_THREADS = (SP_PRODUCER_WARPS + 1 + 4) * 32;   // 544
 constexpr int A_PLANE = SP_TM * SP_TK * 2;                     // bytes of one BF16 plane of A
 constexpr int B_PLANE = SP_TN * SP_TK * 2;                     // ... of B
 constexpr int STAGE_BYTES = 6 * A_PLANE + 6 * B_PLANE;         // 36,864
-constexpr int SMEM_BYTES = SP_STAGES * STAGE_BYTES + 128;      // + mbarriers, TMEM slot
-constexpr uint32_t TMEM_COLS = 2 * SP_TN;                      // Cr | Ci, FP32
+constexpr int SMEM_BYTES = SP_STAGES * STAGE_BYTES + 256;      // + mbarriers, TMEM slot, abort flag
+constexpr uint32_t TMEM_COLS = 4 * SP_TN;                      // two accumulators (Cr | Ci), FP32
 constexpr long long WAIT_LIMIT = 1ll << 20;
 
 // instruction descriptor, kind::f16: D f32, A/B bf16, both K-major, N>>3, M>>4
@@ -76,8 +84,11 @@ __device__ __forceinline__ void umma_commit(uint32_t bar) {
                : "memory");
 }
 
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+// Bounded wait on an mbarrier phase; gives up early when another role of the
+// CTA has raised the abort flag.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int* abort_flag) {
   for (long long i = 0; i < WAIT_LIMIT; ++i) {
+    if (abort_flag && (i & 1023) == 1023 && *abort_flag) return false;
     uint32_t done;
     asm volatile(
         "{\n\t"
@@ -149,24 +160,168 @@ __device__ __forceinline__ void store_chunk(unsigned char* planes, int plane_byt
 // byte offset of the chunk (row r, k-chunk kc) inside a plane
 __device__ __forceinline__ int chunk_off(int r, int kc) { return (r >> 3) * 256 + kc * 128 + (r & 7) * 16; }
 
-__global__ void __launch_bounds__(SP_THREADS, 2)
-grouped_zgemm_split_kernel(const GJob* __restrict__ jobs, const GGroup* __restrict__ groups,
+// Steps of one CTA: its jobs (blockIdx.x, +gridDim.x, ...), their GEMM terms and
+// K=16 steps, in the order every role walks them.  Holds only what a
+// producer's loads need.
+struct StepIter {
+  const GJob* jobs;
+  const GGroup* groups;
+  const GTerm* terms;
+  const Bases* bases;
+  int njobs, jb;          // current job (global index)
+  int t1, ti, kk, nk;     // job's term end, current term, its step, its steps
+  int m0, n0, M, N;       // tile origin and group extent
+  const double2* L;       // current term
+  const double2* R;
+  int l_ld, r_ld, K;
+  bool l_conj, l_n, r_conj, r_n;
+  double ar, ai;
+  bool valid;
+
+  __device__ bool load_term(int i) {
+    const GTerm t = terms[i];
+    if (t.kind != TK_GEMM || t.K <= 0) return false;
+    L = bases->p[t.l_base] + t.l_off;
+    R = bases->p[t.r_base] + t.r_off;
+    l_ld = t.l_ld;
+    r_ld = t.r_ld;
+    K = t.K;
+    l_n = t.l_op == OP_N;
+    l_conj = t.l_op == OP_C;
+    r_n = t.r_op == OP_N;
+    r_conj = t.r_op == OP_C;
+    ar = t.ar;
+    ai = t.ai;
+    kk = 0;
+    nk = (t.K + SP_TK - 1) / SP_TK;
+    return true;
+  }
+  __device__ void first_job(int j) {
+    valid = false;
+    for (jb = j; jb < njobs; jb += gridDim.x) {
+      const GJob job = jobs[jb];
+      const GGroup g = groups[job.group];
+      m0 = job.tm * SP_TM;
+      n0 = job.tn * SP_TN;
+      M = g.M;
+      N = g.N;
+      t1 = job.t1;
+      for (ti = job.t0; ti < t1; ++ti)
+        if (load_term(ti)) {
+          valid = true;
+          return;
+        }
+    }
+  }
+  __device__ void init(const GJob* j_, const GGroup* g_, const GTerm* t_, const Bases* b_, int n) {
+    jobs = j_;
+    groups = g_;
+    terms = t_;
+    bases = b_;
+    njobs = n;
+    first_job(blockIdx.x);
+  }
+  __device__ void next() {
+    if (++kk < nk) return;
+    for (++ti; ti < t1; ++ti)
+      if (load_term(ti)) return;
+    first_job(jb + gridDim.x);
+  }
+};
+
+// loads this thread's chunk of the current step: 8 consecutive k of one row of
+// op(L) (chunks 0..255) or of one column of op(R) (chunks 256..383), raw
+__device__ __forceinline__ void load_chunk(const StepIter& it, int chunk, double2* v) {
+  if (chunk < 256) {
+    const int r = chunk & 127, kc = chunk >> 7;
+    const int gi = it.m0 + r, kb = it.kk * SP_TK + kc * 8;
+#pragma unroll
+    for (int e = 0; e < 8; ++e) {
+      const int k = kb + e;
+      double2 x = make_double2(0.0, 0.0);
+      if (gi < it.M && k < it.K)
+        x = it.l_n ? it.L[(long long)gi + (long long)k * it.l_ld] : it.L[(long long)k + (long long)gi * it.l_ld];
+      v[e] = x;
+    }
+  } else {
+    const int c = (chunk - 256) & 63, kc = (chunk - 256) >> 6;
+    const int gj = it.n0 + c, kb = it.kk * SP_TK + kc * 8;
+#pragma unroll
+    for (int e = 0; e < 8; ++e) {
+      const int k = kb + e;
+      double2 x = make_double2(0.0, 0.0);
+      if (gj < it.N && k < it.K)
+        x = it.r_n ? it.R[(long long)k + (long long)gj * it.r_ld] : it.R[(long long)gj + (long long)k * it.r_ld];
+      v[e] = x;
+    }
+  }
+}
+
+// conj / alpha of a loaded chunk, then its slices into the stage
+__device__ __forceinline__ void store_loaded(bool conj, double ar, double ai, int chunk, unsigned char* st,
+                                             double2* v) {
+  if (chunk < 256) {
+    if (conj)
+#pragma unroll
+      for (int e = 0; e < 8; ++e) v[e].y = -v[e].y;
+    store_chunk(st, A_PLANE, chunk_off(chunk & 127, chunk >> 7), v);
+  } else {
+#pragma unroll
+    for (int e = 0; e < 8; ++e) {
+      const double xr = v[e].x, xi = conj ? -v[e].y : v[e].y;
+      v[e] = make_double2(ar * xr - ai * xi, ar * xi + ai * xr);
+    }
+    const int c = (chunk - 256) & 63, kc = (chunk - 256) >> 6;
+    store_chunk(st + 6 * A_PLANE, B_PLANE, chunk_off(c, kc), v);
+  }
+}
+
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+
+// number of K=16 steps of a job (0: only element terms)
+__device__ __forceinline__ int job_steps(const GJob& job, const GTerm* terms) {
+  int n = 0;
+  for (int ti = job.t0; ti < job.t1; ++ti) {
+    const GTerm t = terms[ti];
+    if (t.kind == TK_GEMM && t.K > 0) n += (t.K + SP_TK - 1) / SP_TK;
+  }
+  return n;
+}
+
+// Persistent, warp-specialised: warps 0..11 produce stages (one chunk per
+// thread per step, the next step's loads in flight while the current one is
+// converted), warp 12 issues the MMAs (one elected lane) into one of two TMEM
+// accumulators, warps 13..16 drain the other accumulator into the outputs.
+__global__ void __launch_bounds__(SP_THREADS, 1)
+grouped_zgemm_split_kernel(const GJob* __restrict__ jobs, int njobs, const GGroup* __restrict__ groups,
                            const GTerm* __restrict__ terms, Bases bases) {
   extern __shared__ __align__(1024) unsigned char smem[];
-  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + SP_STAGES * STAGE_BYTES);
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smem + SP_STAGES * STAGE_BYTES + 64);
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + SP_STAGES * STAGE_BYTES);
+  uint64_t* empty = full + SP_STAGES;
+  uint64_t* accf = empty + SP_STAGES;
+  uint64_t* acce = accf + 2;
+  uint64_t* fin = acce + 2;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(fin + 1);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const GJob job = jobs[blockIdx.x];
-  const GGroup g = groups[job.group];
-  const int m0 = job.tm * SP_TM, n0 = job.tn * SP_TN;
 
   if (tid == 0) {
-    for (int s = 0; s < SP_STAGES; ++s)
-      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&bars[s])) : "memory");
+    for (int s = 0; s < SP_STAGES; ++s) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&full[s])), "r"(SP_PRODUCER_WARPS) : "memory");
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&empty[s])) : "memory");
+    }
+    for (int a = 0; a < 2; ++a) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&accf[a])) : "memory");
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&acce[a])), "r"(4) : "memory");
+    }
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(fin)) : "memory");
+    *abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   __syncwarp();
-  if (warp == 0) {
+  if (warp == SP_MMA_WARP) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
                  "r"(TMEM_COLS)
                  : "memory");
@@ -177,160 +332,177 @@ grouped_zgemm_split_kernel(const GJob* __restrict__ jobs, const GGroup* __restri
   fence_after_sync();
   const uint32_t tmem = *tmem_slot;
 
-  // ---- main loop over the GEMM terms, one K=16 step per pipeline stage -----
-  int q = 0;   // steps issued
-  bool fault = false;
-  for (int ti = job.t0; ti < job.t1 && !fault; ++ti) {
-    const GTerm t = terms[ti];
-    if (t.kind != TK_GEMM) continue;
-    const double2* L = bases.p[t.l_base] + t.l_off;
-    const double2* R = bases.p[t.r_base] + t.r_off;
-    const int nk = (t.K + SP_TK - 1) / SP_TK;
-    for (int kk = 0; kk < nk; ++kk, ++q) {
+  auto fail = [&]() {
+    *abort_flag = 1;
+    atomicExch(&g_split_fault, 1);
+  };
+
+  if (warp < SP_PRODUCER_WARPS) {
+    // ---------------------------------------------------------------- producers
+    StepIter it;
+    it.init(jobs, groups, terms, &bases, njobs);
+    double2 nxt[8];
+    if (it.valid) load_chunk(it, tid, nxt);
+    for (int q = 0; it.valid; ++q) {
+      double2 cur[8];
+#pragma unroll
+      for (int e = 0; e < 8; ++e) cur[e] = nxt[e];
+      const bool conj = tid < 256 ? it.l_conj : it.r_conj;
+      const double ar = it.ar, ai = it.ai;
       const int s = q % SP_STAGES;
-      unsigned char* st = smem + s * STAGE_BYTES;
-      // the MMAs of step q - STAGES must have finished reading this stage
-      const bool ok = q < SP_STAGES || mbar_wait(smem_u32(&bars[s]), (uint32_t)((q / SP_STAGES - 1) & 1));
-      // A: op(L), 128 rows x 16 k -> 256 chunks of 8 k, one per thread
-      {
-        const int r = tid & 127, kc = tid >> 7;
-        const int gi = m0 + r, kb = kk * SP_TK + kc * 8;
-        double2 v[8];
-#pragma unroll
-        for (int e = 0; e < 8; ++e) {
-          const int k = kb + e;
-          double2 x = make_double2(0.0, 0.0);
-          if (gi < g.M && k < t.K) {
-            x = (t.l_op == OP_N) ? L[(long long)gi + (long long)k * t.l_ld] : L[(long long)k + (long long)gi * t.l_ld];
-            if (t.l_op == OP_C) x.y = -x.y;
-          }
-          v[e] = x;
-        }
-        store_chunk(st, A_PLANE, chunk_off(r, kc), v);
-      }
-      // B: alpha * op(R), 16 k x 64 columns -> 128 chunks, threads 0..127
-      if (tid < 128) {
-        const int c = tid & 63, kc = tid >> 6;
-        const int gj = n0 + c, kb = kk * SP_TK + kc * 8;
-        double2 v[8];
-#pragma unroll
-        for (int e = 0; e < 8; ++e) {
-          const int k = kb + e;
-          double2 x = make_double2(0.0, 0.0);
-          if (gj < g.N && k < t.K) {
-            x = (t.r_op == OP_N) ? R[(long long)k + (long long)gj * t.r_ld] : R[(long long)gj + (long long)k * t.r_ld];
-            if (t.r_op == OP_C) x.y = -x.y;
-          }
-          v[e] = make_double2(t.ar * x.x - t.ai * x.y, t.ar * x.y + t.ai * x.x);
-        }
-        store_chunk(st + 6 * A_PLANE, B_PLANE, chunk_off(c, kc), v);
-      }
-      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-      if (__syncthreads_or(!ok)) {   // block-uniform decision
-        fault = true;
+      it.next();
+      if (it.valid) load_chunk(it, tid, nxt);   // in flight while this step converts
+      if (q >= SP_STAGES && !mbar_wait(smem_u32(&empty[s]), (uint32_t)((q / SP_STAGES - 1) & 1), abort_flag)) {
+        fail();
         break;
       }
-      if (tid == 0) {
-        fence_after_sync();
-        const uint32_t a0 = smem_u32(st), b0 = smem_u32(st + 6 * A_PLANE);
-#pragma unroll
-        for (int pi = 0; pi < 6; ++pi) {
-          const int sa = c_pairs[pi][0], sb = c_pairs[pi][1];
-          const uint64_t ar = smem_desc(a0 + (2 * sa) * A_PLANE), ai = smem_desc(a0 + (2 * sa + 1) * A_PLANE);
-          const uint64_t br = smem_desc(b0 + (2 * sb) * B_PLANE), bi = smem_desc(b0 + (2 * sb + 1) * B_PLANE);
-          const uint32_t first = (q == 0 && pi == 0) ? 0u : 1u;
-          umma_bf16(tmem, ar, br, IDESC, first);                  // Cr  = Ar Br
-          umma_bf16(tmem, ai, bi, IDESC_NEG_A, 1u);               // Cr -= Ai Bi
-          umma_bf16(tmem + SP_TN, ar, bi, IDESC, first);          // Ci  = Ar Bi
-          umma_bf16(tmem + SP_TN, ai, br, IDESC, 1u);             // Ci += Ai Br
-        }
-        umma_commit(smem_u32(&bars[s]));
-      }
-    }
-  }
-  // all MMAs of this CTA are complete once the last committed stage arrives
-  if (q > 0) {
-    const int s = (q - 1) % SP_STAGES;
-    if (!mbar_wait(smem_u32(&bars[s]), (uint32_t)(((q - 1) / SP_STAGES) & 1))) fault = true;
-  }
-  fault = __syncthreads_or(fault);
-  fence_after_sync();
-
-  if (!fault) {
-    // ---- epilogue: warp w reads TMEM lanes 32*(w%4).., column half w/4 --------
-    const int quad = warp & 3, half = warp >> 2;
-    const int row = m0 + quad * 32 + lane;
-    const uint32_t lane_base = tmem + ((uint32_t)(quad * 32) << 16);
-    const bool partial = job.part >= 0;
-    double2* C = partial ? bases.part + job.part_off : bases.p[g.c_base] + g.c_off;
-    const long long ldc = partial ? g.M : g.c_ld;
-    const bool acc_old = !partial && g.beta;
-#pragma unroll 1
-    for (int cb = 0; cb < 2; ++cb) {
-      const int c0 = half * 32 + cb * 16;
-      float vr[16], vi[16];
+      store_loaded(conj, ar, ai, tid, smem + s * STAGE_BYTES, cur);
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       __syncwarp();
-      if (q > 0) {
-        tmem_ld16(lane_base + c0, vr);
-        tmem_ld16(lane_base + SP_TN + c0, vi);
-      } else {
-#pragma unroll
-        for (int j = 0; j < 16; ++j) vr[j] = vi[j] = 0.f;
-      }
-      double cr[16], ci[16];
-#pragma unroll
-      for (int j = 0; j < 16; ++j) {
-        cr[j] = vr[j];
-        ci[j] = vi[j];
-      }
-      // element terms (AXPY / DIAG) in FP64, as grouped_zgemm applies them
-      for (int ti = job.t0; ti < job.t1; ++ti) {
-        const GTerm t = terms[ti];
-        if (t.kind == TK_GEMM) continue;
-        const double2* R = bases.p[t.r_base] + t.r_off;
-        const int rr = row - t.r0;
-        if (row >= g.M || rr < 0 || rr >= t.rm) continue;
-#pragma unroll
-        for (int j = 0; j < 16; ++j) {
-          const int col = n0 + c0 + j, cc = col - t.c0;
-          if (col >= g.N || cc < 0 || cc >= t.rn) continue;
-          double xr, xi;
-          if (t.kind == TK_AXPY) {
-            const double2 x = (t.r_op == OP_N) ? R[(long long)rr + (long long)cc * t.r_ld]
-                                               : R[(long long)cc + (long long)rr * t.r_ld];
-            xr = x.x;
-            xi = (t.r_op == OP_C) ? -x.y : x.y;
-          } else {
-            if (rr != cc) continue;
-            xr = 1.0;
-            xi = 0.0;
-          }
-          cr[j] += t.ar * xr - t.ai * xi;
-          ci[j] += t.ar * xi + t.ai * xr;
-        }
-      }
-      if (row < g.M) {
-#pragma unroll
-        for (int j = 0; j < 16; ++j) {
-          const int col = n0 + c0 + j;
-          if (col >= g.N) continue;
-          double2* p = C + (long long)row + (long long)col * ldc;
-          double2 v = make_double2(cr[j], ci[j]);
-          if (acc_old) {
-            const double2 o = *p;
-            v.x += o.x;
-            v.y += o.y;
-          }
-          *p = v;
-        }
-      }
+      if (lane == 0) mbar_arrive(smem_u32(&full[s]));
     }
-  } else if (tid == 0) {
-    atomicExch(&g_split_fault, 1);
+  } else if (warp == SP_MMA_WARP) {
+    // ---------------------------------------------------------------- MMA issuer
+    if (lane == 0) {
+      int q = 0, jl = 0;
+      bool ok = true;
+      for (int jb = blockIdx.x; jb < njobs && ok; jb += gridDim.x) {
+        const int nst = job_steps(jobs[jb], terms);
+        if (nst == 0) continue;
+        const int a = jl & 1, ua = jl >> 1;
+        if (ua >= 1 && !mbar_wait(smem_u32(&acce[a]), (uint32_t)((ua - 1) & 1), abort_flag)) {
+          ok = false;
+          break;
+        }
+        fence_after_sync();
+        const uint32_t dcr = tmem + a * (2 * SP_TN), dci = dcr + SP_TN;
+        for (int i = 0; i < nst; ++i, ++q) {
+          const int s = q % SP_STAGES;
+          if (!mbar_wait(smem_u32(&full[s]), (uint32_t)((q / SP_STAGES) & 1), abort_flag)) {
+            ok = false;
+            break;
+          }
+          fence_after_sync();
+          const uint32_t a0 = smem_u32(smem + s * STAGE_BYTES), b0 = a0 + 6 * A_PLANE;
+#pragma unroll
+          for (int pi = 0; pi < 6; ++pi) {
+            const int sa = c_pairs[pi][0], sb = c_pairs[pi][1];
+            const uint64_t ar = smem_desc(a0 + (2 * sa) * A_PLANE), ai = smem_desc(a0 + (2 * sa + 1) * A_PLANE);
+            const uint64_t br = smem_desc(b0 + (2 * sb) * B_PLANE), bi = smem_desc(b0 + (2 * sb + 1) * B_PLANE);
+            const uint32_t first = (i == 0 && pi == 0) ? 0u : 1u;
+            umma_bf16(dcr, ar, br, IDESC, first);          // Cr  = Ar Br
+            umma_bf16(dcr, ai, bi, IDESC_NEG_A, 1u);       // Cr -= Ai Bi
+            umma_bf16(dci, ar, bi, IDESC, first);          // Ci  = Ar Bi
+            umma_bf16(dci, ai, br, IDESC, 1u);             // Ci += Ai Br
+          }
+          umma_commit(smem_u32(&empty[s]));
+        }
+        if (!ok) break;
+        umma_commit(smem_u32(&accf[a]));
+        jl++;
+      }
+      if (!ok) fail();
+      // every MMA issued here has completed before the accumulators are freed
+      umma_commit(smem_u32(fin));
+      if (!mbar_wait(smem_u32(fin), 0u, nullptr)) fail();
+    }
+    __syncwarp();
+  } else {
+    // ---------------------------------------------------------------- epilogue
+    const int ew = warp - SP_EPI_WARP0;      // 0..3
+    const int quad = warp & 3;               // TMEM lane quadrant this warp may read
+    int jl = 0;
+    for (int jb = blockIdx.x; jb < njobs; jb += gridDim.x) {
+      const GJob job = jobs[jb];
+      const GGroup g = groups[job.group];
+      const int nst = job_steps(job, terms);
+      const int a = jl & 1, ua = jl >> 1;
+      if (nst > 0) {
+        if (!mbar_wait(smem_u32(&accf[a]), (uint32_t)(ua & 1), abort_flag)) {
+          fail();
+          break;
+        }
+        fence_after_sync();
+      }
+      const int m0 = job.tm * SP_TM, n0 = job.tn * SP_TN;
+      const int row = m0 + quad * 32 + lane;
+      const uint32_t lane_base = tmem + a * (2 * SP_TN) + ((uint32_t)(quad * 32) << 16);
+      const bool partial = job.part >= 0;
+      double2* C = partial ? bases.part + job.part_off : bases.p[g.c_base] + g.c_off;
+      const long long ldc = partial ? g.M : g.c_ld;
+      const bool acc_old = !partial && g.beta;
+#pragma unroll 1
+      for (int cb = 0; cb < SP_TN / 16; ++cb) {
+        const int c0 = cb * 16;
+        float vr[16], vi[16];
+        __syncwarp();
+        if (nst > 0) {
+          tmem_ld16(lane_base + c0, vr);
+          tmem_ld16(lane_base + SP_TN + c0, vi);
+        } else {
+#pragma unroll
+          for (int j = 0; j < 16; ++j) vr[j] = vi[j] = 0.f;
+        }
+        if (nst > 0 && cb == SP_TN / 16 - 1) {   // accumulator read out: hand it back
+          fence_before_sync();
+          __syncwarp();
+          if (lane == 0) mbar_arrive(smem_u32(&acce[a]));
+        }
+        double cr[16], ci[16];
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+          cr[j] = vr[j];
+          ci[j] = vi[j];
+        }
+        // element terms (AXPY / DIAG) in FP64, as grouped_zgemm applies them
+        for (int ti = job.t0; ti < job.t1; ++ti) {
+          const GTerm t = terms[ti];
+          if (t.kind == TK_GEMM) continue;
+          const double2* R = bases.p[t.r_base] + t.r_off;
+          const int rr = row - t.r0;
+          if (row >= g.M || rr < 0 || rr >= t.rm) continue;
+#pragma unroll
+          for (int j = 0; j < 16; ++j) {
+            const int col = n0 + c0 + j, cc = col - t.c0;
+            if (col >= g.N || cc < 0 || cc >= t.rn) continue;
+            double xr, xi;
+            if (t.kind == TK_AXPY) {
+              const double2 x = (t.r_op == OP_N) ? R[(long long)rr + (long long)cc * t.r_ld]
+                                                 : R[(long long)cc + (long long)rr * t.r_ld];
+              xr = x.x;
+              xi = (t.r_op == OP_C) ? -x.y : x.y;
+            } else {
+              if (rr != cc) continue;
+              xr = 1.0;
+              xi = 0.0;
+            }
+            cr[j] += t.ar * xr - t.ai * xi;
+            ci[j] += t.ar * xi + t.ai * xr;
+          }
+        }
+        if (row < g.M) {
+#pragma unroll
+          for (int j = 0; j < 16; ++j) {
+            const int col = n0 + c0 + j;
+            if (col >= g.N) continue;
+            double2* p = C + (long long)row + (long long)col * ldc;
+            double2 v = make_double2(cr[j], ci[j]);
+            if (acc_old) {
+              const double2 o = *p;
+              v.x += o.x;
+              v.y += o.y;
+            }
+            *p = v;
+          }
+        }
+      }
+      if (nst > 0) jl++;
+      (void)ew;
+    }
   }
   fence_before_sync();
   __syncthreads();
-  if (warp == 0) {
+  if (warp == SP_MMA_WARP) {
     fence_after_sync();
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS) : "memory");
   }
@@ -348,7 +520,15 @@ cudaError_t launch_grouped_zgemm_split(const GJob* jobs, int njobs, const GGroup
     if (e != cudaSuccess) return e;
     attr_set = true;
   }
-  grouped_zgemm_split_kernel<<<njobs, SP_THREADS, SMEM_BYTES, st>>>(jobs, groups, terms, bases);
+  static int nsm = 0;
+  if (!nsm) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    if (nsm <= 0) nsm = 148;
+  }
+  const int grid = njobs < nsm ? njobs : nsm;
+  grouped_zgemm_split_kernel<<<grid, SP_THREADS, SMEM_BYTES, st>>>(jobs, njobs, groups, terms, bases);
   return cudaGetLastError();
 }
 
