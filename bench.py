@@ -12,7 +12,9 @@ blocks), identical for every arm.  A step is one H.psi application.
 
 Prints one JSON line (rank 0).  value = algorithmic TFLOP/s (flops counted in
 the reference's GEMM association order, 8*m*n*k per complex GEMM) of all ranks;
-N>1 runs independent replicas (the path does not shard).
+N>1 runs independent replicas (the path does not shard).  Rank 0 adds the
+split-precision form on the same superblock ("split") and the whole YC4x12
+ground-state search in both forms ("sweep": seconds per sweep, energies).
 """
 from __future__ import annotations
 
@@ -38,10 +40,68 @@ WORKLOAD = ("YC4x12 (48 sites, 44 e-, S=0, t1=1 t2=0.3 J1=0.4 J2=0.036) superblo
 
 
 # ----------------------------------------------------------------------------- workload
-def make_superblock(seed=SEED):
+def scale_dims(ints, k):
+    """The same descriptors with every matrix dimension (block, sector, piece
+    offset and width, psi sector) multiplied by k: the sector structure of the
+    m=1000 superblock at k^2 the size (k=4: m ~ 4000, the size class of YC4x24 at
+    m=4000, 64x the flops per H.psi)."""
+    if k == 1:
+        return ints
+    x = ints.astype(np.int64).copy()
+    i = 0
+
+    def block():
+        nonlocal i
+        num = x[i + 1]
+        x[i + 2] *= k
+        i += 5
+        for _ in range(num):
+            x[i + 3] *= k
+            x[i + 4] *= k
+            i += 5
+
+    def model():
+        nonlocal i
+        nops = x[i + 1]
+        i += 2
+        block()
+        for _ in range(4 * nops):
+            block()
+
+    def basis():
+        nonlocal i
+        num = x[i + 1]
+        x[i + 2] *= k
+        i += 3
+        npc = 0
+        for _ in range(num):
+            x[i + 2] *= k
+            npc += x[i + 3]
+            i += 4
+        for _ in range(npc):
+            x[i + 4] *= k
+            x[i + 5] *= k
+            i += 6
+
+    model()
+    model()
+    basis()
+    basis()
+    num = x[i + 2]
+    x[i + 3] *= k * k
+    i += 4
+    for _ in range(num):
+        x[i + 4] *= k
+        x[i + 5] *= k
+        i += 6
+    assert i == len(x)
+    return x.astype(np.int32)
+
+
+def make_superblock(seed=SEED, scale=1):
     """Fixture descriptors + seeded values -> (sys_len, env_len, ints, data, psi_offset, n)."""
     z = np.load(FIXTURE)
-    ints = z["ints"].astype(np.int32)
+    ints = scale_dims(z["ints"].astype(np.int32), scale)
     rng = np.random.default_rng(seed)
     chunks = []
     i = 0
@@ -216,6 +276,89 @@ def run_reference(args):
     return 0
 
 
+def measured_bf16_peak():
+    """Burst cuBLAS bf16 TFLOP/s measured on this pool (MEASURED_PEAKS.json), else the fallback."""
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["bf16_tflops"]), "MEASURED_PEAKS.json bf16_tflops (burst)"
+    except (OSError, KeyError, ValueError):
+        return 1590.0, "fallback 1.59 PFLOP/s"
+
+
+def split_leg(torch, dev, sb, steps, fp64_out):
+    """The split-precision form (BF16 slices on tcgen05) on the same superblock and psi."""
+    from tsc_tri_t1t2j1j2_b200 import Context
+    sl, el, ints, data, off, n = sb
+    ctx = Context(device=dev.index, **MODEL)
+    ctx.set_precision(Context.SPLIT_BF16)
+    ctx.set_superblock_flat(sl, el, ints, data)
+    stream = torch.cuda.ExternalStream(ctx.stream, device=dev)
+    psi = torch.from_numpy(data[off:off + n].copy()).to(dev)
+    out = torch.empty_like(psi)
+    torch.cuda.synchronize()
+    for _ in range(3):
+        ctx.hpsi_device(psi.data_ptr(), out.data_ptr())
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        ctx.hpsi_device(psi.data_ptr(), out.data_ptr())
+    e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    st = ctx.hpsi_stats()
+    ctx.close()
+    got = out.cpu().numpy()
+    err = float(np.max(np.abs(got - fp64_out)) / np.max(np.abs(fp64_out)))
+    # tensor work the kernel executes: 6 slice products x 4 real parts per complex
+    # multiply-add, 2 flops each = 6x the complex flops of the task list
+    bf16_flops = 6.0 * st["exec_flops"]
+    peak, src = measured_bf16_peak()
+    achieved = bf16_flops / (ms * 1e-3) / 1e12
+    return {"hpsi_tflops": st["ref_flops"] / (ms * 1e-3) / 1e12, "ms_per_hpsi": ms,
+            "max_rel_err_vs_fp64": err, "tolerance": 2e-5,
+            "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                         "frac": achieved / peak, "peak_source": src,
+                         "note": "BF16 tensor flops executed (6x the task list's complex flops)",
+                         "kernel": "grouped_zgemm_split (tcgen05, 2 launches per H.psi)"}}
+
+
+SWEEP_CONFIG = dict(kept_min=200, kept_warm=200, sweeps=[200, 400, 600, 800, 1000, 1000], lanzero=1e-10)
+
+
+def sweep_leg(dev):
+    """Whole ground-state search of YC4x12 (48 sites, m ramped to 1000 over 6 sweeps)
+    on the device in both forms: seconds of the warm-up and of the sweeps, the
+    final energies and their relative difference."""
+    from tsc_tri_t1t2j1j2_b200 import Context
+    res = {"workload": "YC4x12 t1=1 t2=0.3 J1=0.4 J2=0.036, warm-up m=200, 6 sweeps m=200,400,600,800,1000,1000, "
+                       "lanzero 1e-10, random start seed 1"}
+    for name, mode in (("fp64", Context.FP64), ("split", Context.SPLIT_BF16)):
+        ctx = Context(device=dev.index, **MODEL)
+        ctx.set_precision(mode, 1e-11)
+        t0 = time.perf_counter()
+        steps = ctx.get_ground_state(**SWEEP_CONFIG)
+        wall = time.perf_counter() - t0
+        ctx.close()
+        sw = [s for s in steps if s["phase"] != 0]
+        res[name] = {
+            "total_seconds": wall,
+            "warmup_seconds": sum(s["step_seconds"] for s in steps if s["phase"] == 0),
+            "sweep_seconds": sum(s["step_seconds"] for s in sw),
+            "seconds_per_sweep": sum(s["step_seconds"] for s in sw) / (len(SWEEP_CONFIG["sweeps"]) + 1),
+            "lanczos_seconds": sum(s["lanczos_seconds"] for s in sw),
+            "hpsi_seconds": sum(s["hpsi_seconds"] for s in sw),
+            "lanczos_iters": int(sum(s["lanczos_iters"] for s in sw)),
+            "split_iters": int(sum(s["split_iters"] for s in sw)),
+            "final_e0": steps[-1]["e0"],
+            "min_e0": min(s["e0"] for s in steps),
+        }
+    res["final_dE_over_E_split_vs_fp64"] = abs(res["split"]["final_e0"] - res["fp64"]["final_e0"]) / abs(
+        res["fp64"]["final_e0"])
+    res["sweep_speedup_split_over_fp64"] = res["fp64"]["sweep_seconds"] / res["split"]["sweep_seconds"]
+    return res
+
+
 def run_gpu(args):
     import torch
     from tsc_tri_t1t2j1j2_b200 import Context
@@ -227,7 +370,7 @@ def run_gpu(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
-    sb = make_superblock()
+    sb = make_superblock(scale=args.scale)
     sl, el, ints, data, off, n = sb
     ctx = Context(device=local, **MODEL)
     ctx.set_superblock_flat(sl, el, ints, data)
@@ -292,19 +435,24 @@ def run_gpu(args):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128",
             "data": "synthetic: engine-recorded sector structure (tests/golden/superblock_yc4x12_m1000.npz), "
                     "seeded N(0,1) complex values",
-            "config": {"workload": WORKLOAD, "psi_amplitudes": n, "operator_elements": int(off),
+            "config": {"workload": WORKLOAD if args.scale == 1 else
+                       WORKLOAD + f"; every dimension scaled x{args.scale} (synthetic m ~ {1000 * args.scale} size class)",
+                       "psi_amplitudes": n, "operator_elements": int(off),
                        "ref_gflop_per_step": ref_flops / 1e9, "exec_gflop_per_step": exec_flops / 1e9,
-                       "parallelism": f"replicas x{ws}", "cache": "inputs > L2 (operators 254 MB)"},
+                       "parallelism": f"replicas x{ws}", "cache": f"inputs > L2 (operators {16 * off / 1e6:.0f} MB)"},
             "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                         "frac": achieved / peak, "traffic": TRAFFIC_BYTES_PER_STEP,
+                         "frac": achieved / peak, "traffic": TRAFFIC_BYTES_PER_STEP if args.scale == 1 else None,
                          "peak_source": "cuBLAS ZGEMM 4096^3 complex128 measured in this run (FP64 DMMA)",
                          "kernel": "grouped_zgemm (2 launches per H.psi)"},
             "e2e": {"value": e2e, "unit": "TFLOP/s", "h2d_bytes_per_step": 16 * n, "d2h_bytes_per_step": 16 * n},
             "gpu_launches": 2 * args.steps,
             "clocks": clocks.summary(),
         }
+        gpu_out = out.cpu().numpy()
+        line["split"] = split_leg(torch, dev, sb, max(20, args.steps // 4), gpu_out)
+        if not args.no_sweep:
+            line["sweep"] = sweep_leg(dev)
         if ws == 1 and not args.no_cpu:
-            gpu_out = out.cpu().numpy()
             cpu_out, sec, flops, wall = cpu_hpsi(sb, 1)
             err = float(np.max(np.abs(gpu_out - cpu_out)) / np.max(np.abs(cpu_out)))
             line["cpu_baseline"] = {"value": flops / sec / 1e12, "unit": "TFLOP/s", "cores": os.cpu_count(),
@@ -334,6 +482,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-sweep", action="store_true", help="skip the whole-run (sweep seconds) leg")
+    ap.add_argument("--scale", type=int, default=1,
+                    help="multiply every dimension of the superblock by this (4: m ~ 4000 size class)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -33,11 +33,13 @@ void cuda_check(cudaError_t e, const char* what);
 // Device buffer of complex elements, stream-ordered on `st`.  Buffers are carved
 // from per-stream arenas (chunks of the device pool, best fit, coalesced on
 // free), so a DMRG step makes no driver calls once its arena has grown;
-// release_stream_cache() hands a stream's chunks back to the pool.
+// blocks of 64 MiB and more come from the pool directly, which reuses them
+// across sizes; release_stream_cache() hands a stream's chunks back to the pool.
 struct DevBuf {
   double2* p = nullptr;
   size_t n = 0;   // complex elements
   size_t cls = 0; // bytes of the arena block behind p
+  bool direct = false;   // allocated from the pool itself (large blocks)
   cudaStream_t st = nullptr;
   DevBuf() = default;
   DevBuf(size_t count, cudaStream_t s, bool zero);

@@ -113,6 +113,7 @@ std::unordered_map<cudaStream_t, Arena> g_arena;
 constexpr size_t kAlign = 256;
 constexpr size_t kMinChunk = 64ull << 20;
 constexpr size_t kMaxChunk = 4ull << 30;
+constexpr size_t kDirect = 64ull << 20;   // blocks at least this large bypass the arenas
 }  // namespace
 
 void release_stream_cache(cudaStream_t s) {
@@ -126,7 +127,10 @@ void release_stream_cache(cudaStream_t s) {
 DevBuf::DevBuf(size_t count, cudaStream_t s, bool zero) : n(count), st(s) {
   if (count == 0) return;
   cls = (count * sizeof(double2) + kAlign - 1) / kAlign * kAlign;
-  {
+  if (cls >= kDirect) {   // large blocks come straight from the pool, which reuses them across sizes
+    cuda_check(cudaMallocFromPoolAsync((void**)&p, cls, device_pool(), s), "cudaMallocFromPoolAsync");
+    direct = true;
+  } else {
     std::lock_guard<std::mutex> lock(g_arena_mu);
     Arena& A = g_arena[s];
     char* q = A.take(cls);
@@ -152,6 +156,10 @@ DevBuf::DevBuf(size_t count, cudaStream_t s, bool zero) : n(count), st(s) {
 }
 DevBuf::~DevBuf() {
   if (!p) return;
+  if (direct) {
+    cudaFreeAsync(p, st);
+    return;
+  }
   std::lock_guard<std::mutex> lock(g_arena_mu);
   auto it = g_arena.find(st);
   if (it != g_arena.end()) it->second.give(reinterpret_cast<char*>(p), cls);
