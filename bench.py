@@ -359,6 +359,37 @@ def sweep_leg(dev):
     return res
 
 
+CONFIG1 = dict(Nx=6, Ny=4, t1=1.0, t2=0.0, J1=0.4, J2=0.0, delta=12)
+CONFIG1_RUN = dict(kept_min=100, kept_warm=100, sweeps=[100, 200, 300, 400], lanzero=1e-10)
+
+
+def config1_leg(dev, with_cpu):
+    """The reference's CPU-runnable case, whole: YC4x6 (24 sites, 22 e-), t1=1, J1=0.4,
+    4 sweeps m=100/200/300/400, lanzero 1e-10 -- on the device in both forms and,
+    with the CPU leg, the oracle (CPU restatement, OpenBLAS on all host cores)."""
+    from tsc_tri_t1t2j1j2_b200 import Context
+    res = {"workload": "YC4x6 t1=1 J1=0.4 t2=J2=0, warm-up m=100, 4 sweeps m=100,200,300,400, lanzero 1e-10"}
+    for name, mode in (("fp64", Context.FP64), ("split", Context.SPLIT_BF16)):
+        ctx = Context(device=dev.index, **CONFIG1)
+        ctx.set_precision(mode, 1e-11)
+        t0 = time.perf_counter()
+        steps = ctx.get_ground_state(**CONFIG1_RUN)
+        res[name] = {"seconds": time.perf_counter() - t0, "steps": len(steps), "final_e0": steps[-1]["e0"]}
+        ctx.close()
+    if with_cpu:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import orc
+        cfg = orc.RunConfig(Nx=6, Ny=4, t1=1.0, t2=0.0, J1=0.4, J2=0.0, kept_min=100, kept_warm=100,
+                            sweeps=[100, 200, 300, 400], lanzero=1e-10)
+        t0 = time.perf_counter()
+        ref = orc.Oracle(cfg).run()
+        sec = time.perf_counter() - t0
+        res["cpu_oracle"] = {"seconds": sec, "cores": os.cpu_count(), "steps": len(ref), "final_e0": ref[-1]["e0"]}
+        res["fp64_final_dE_over_E_vs_oracle"] = abs(res["fp64"]["final_e0"] - ref[-1]["e0"]) / abs(ref[-1]["e0"])
+        res["speedup_fp64_gpu_over_cpu"] = sec / res["fp64"]["seconds"]
+    return res
+
+
 def run_gpu(args):
     import torch
     from tsc_tri_t1t2j1j2_b200 import Context
@@ -452,6 +483,7 @@ def run_gpu(args):
         line["split"] = split_leg(torch, dev, sb, max(20, args.steps // 4), gpu_out)
         if not args.no_sweep:
             line["sweep"] = sweep_leg(dev)
+            line["sweep_config1"] = config1_leg(dev, ws == 1 and not args.no_cpu)
         if ws == 1 and not args.no_cpu:
             cpu_out, sec, flops, wall = cpu_hpsi(sb, 1)
             err = float(np.max(np.abs(gpu_out - cpu_out)) / np.max(np.abs(cpu_out)))

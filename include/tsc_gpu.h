@@ -165,7 +165,7 @@ void* tsc_stream(tsc_ctx* ctx);
  * H.psi); Lanczos iterates on that H.psi until successive Ritz values agree to
  * split_tol relative (<= 0 keeps the current value, 1e-9 at creation), then
  * runs the reference's FP64 iterations from that vector until the FP64
- * residual ||H psi - E psi|| is below sqrt(lanzero), so the energy and
+ * residual ||H psi - E psi|| is below 0.1 sqrt(lanzero), so the energy and
  * vector it returns are FP64 results.  Orthogonalisation, tridiagonal solve,
  * density-matrix eigensolver, renormalisation and wave transforms stay FP64,
  * and so do the warm-up steps of tsc_dmrg_run.  Takes effect from the next

@@ -33,7 +33,7 @@ void cuda_check(cudaError_t e, const char* what);
 // Device buffer of complex elements, stream-ordered on `st`.  Buffers are carved
 // from per-stream arenas (chunks of the device pool, best fit, coalesced on
 // free), so a DMRG step makes no driver calls once its arena has grown;
-// blocks of 64 MiB and more come from the pool directly, which reuses them
+// blocks of 4 GiB and more come from the pool directly, which reuses them
 // across sizes; release_stream_cache() hands a stream's chunks back to the pool.
 struct DevBuf {
   double2* p = nullptr;

@@ -113,7 +113,7 @@ std::unordered_map<cudaStream_t, Arena> g_arena;
 constexpr size_t kAlign = 256;
 constexpr size_t kMinChunk = 64ull << 20;
 constexpr size_t kMaxChunk = 4ull << 30;
-constexpr size_t kDirect = 64ull << 20;   // blocks at least this large bypass the arenas
+constexpr size_t kDirect = 4ull << 30;   // blocks at least this large bypass the arenas
 }  // namespace
 
 void release_stream_cache(cudaStream_t s) {
