@@ -390,6 +390,57 @@ def config1_leg(dev, with_cpu):
     return res
 
 
+def config5_leg(torch, dev, zgemm_peak):
+    """The benchmark list's synthetic block-sparse H.psi (tsc_blocksparse_*): one
+    problem of K=64 sectors, dimensions log-uniform in [16, 2048], 8 left and 8
+    right operator sets with sector shifts in -2..2, 200 terms with alpha ~ U[-1,1];
+    and a batch of 32 independent problems of uneven size (K in 16..64, dimensions
+    in [16, 256]) applied in one pair of launches.  FP64 and split forms, the
+    split form's largest absolute deviation from the FP64 result."""
+    from tsc_tri_t1t2j1j2_b200 import Context
+    from tsc_tri_t1t2j1j2_b200.blocksparse import random_psi, synthetic
+    out = {"workload": "synthetic block-sparse H.psi: entries re/im N(0,1), shift-0 blocks Hermitian; "
+                       "single: K=64 dims log-uniform [16,2048] 8+8 sets 200 terms; "
+                       "batch32: 32 problems K in 16..64 dims [16,256] 8+8 sets 200 terms each, one launch pair"}
+    rng = np.random.default_rng(SEED + 5)
+    cases = {"single": [synthetic(rng, 64, 16, 2048)],
+             "batch32": [synthetic(rng, int(k), 16, 256) for k in rng.integers(16, 65, 32)]}
+    for name, probs in cases.items():
+        ctx = Context(device=dev.index, **MODEL)
+        n, flops, xflops = ctx.blocksparse_set(probs)
+        x = torch.from_numpy(random_psi(rng, probs)).to(dev)
+        ys = {}
+        res = {"problems": len(probs), "psi_amplitudes": n, "gflop_per_application": flops / 1e9,
+               "gflop_executed": xflops / 1e9}
+        stream = torch.cuda.ExternalStream(ctx.stream, device=dev)
+        for form, mode in (("fp64", Context.FP64), ("split", Context.SPLIT_BF16)):
+            y = torch.empty_like(x)
+            torch.cuda.synchronize()
+            for _ in range(2):
+                ctx.blocksparse_apply(x.data_ptr(), y.data_ptr(), mode)
+            torch.cuda.synchronize()
+            reps = 5
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(reps):
+                ctx.blocksparse_apply(x.data_ptr(), y.data_ptr(), mode)
+            e1.record(stream)
+            e1.synchronize()
+            ms = e0.elapsed_time(e1) / reps
+            res[form] = {"ms": ms, "tflops": flops / (ms * 1e-3) / 1e12,
+                         "executed_tflops": xflops / (ms * 1e-3) / 1e12}
+            ys[form] = y.cpu().numpy()
+        res["fp64"]["frac_of_zgemm"] = res["fp64"]["executed_tflops"] / zgemm_peak
+        bf16, _ = measured_bf16_peak()
+        res["split"]["frac_of_bf16"] = 6.0 * res["split"]["executed_tflops"] / bf16
+        res["split_max_abs_err"] = float(np.max(np.abs(ys["split"] - ys["fp64"])))
+        res["split_max_rel_err"] = res["split_max_abs_err"] / float(np.max(np.abs(ys["fp64"])))
+        res["split_speedup"] = res["fp64"]["ms"] / res["split"]["ms"]
+        out[name] = res
+        ctx.close()
+    return out
+
+
 def run_gpu(args):
     import torch
     from tsc_tri_t1t2j1j2_b200 import Context
@@ -481,6 +532,8 @@ def run_gpu(args):
         }
         gpu_out = out.cpu().numpy()
         line["split"] = split_leg(torch, dev, sb, max(20, args.steps // 4), gpu_out)
+        if not args.no_synthetic:
+            line["config5"] = config5_leg(torch, dev, peak)
         if not args.no_sweep:
             line["sweep"] = sweep_leg(dev)
             line["sweep_config1"] = config1_leg(dev, ws == 1 and not args.no_cpu)
@@ -515,6 +568,7 @@ def main():
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-sweep", action="store_true", help="skip the whole-run (sweep seconds) leg")
+    ap.add_argument("--no-synthetic", action="store_true", help="skip the synthetic block-sparse leg")
     ap.add_argument("--scale", type=int, default=1,
                     help="multiply every dimension of the superblock by this (4: m ~ 4000 size class)")
     args = ap.parse_args()

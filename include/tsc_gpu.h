@@ -174,6 +174,29 @@ void* tsc_stream(tsc_ctx* ctx);
 #define TSC_SPLIT_BF16 1
 int tsc_set_precision(tsc_ctx* ctx, int mode, double split_tol);
 
+/* Block-sparse H.psi on a batch of independent problems, all of them in the
+ * same two grouped launches (no counterpart in the reference, which applies
+ * model_wave to one superblock at a time; this is the synthetic H.psi of the
+ * benchmark list).  Problem p has K sectors; its psi is the sector blocks X_i
+ * (d_i x e_i, column-major) one after another, problems one after another, and
+ * the output has the same layout.  Left operator sets L_a hold blocks L_a[i]
+ * (d_{i+s_a} x d_i), right sets R_b blocks R_b[i] (e_{i+s_b} x e_i), for every i
+ * with 0 <= i+s < K.  A term (alpha, a, b), s_a == s_b, adds
+ * alpha * L_a[i] X_i R_b[i]^H to Y_{i+s}; sectors no term reaches are zero.
+ *   ints, per problem: K, nL, nR, nterms; d_0, e_0, ..., d_{K-1}, e_{K-1};
+ *        the shifts s of the left then right sets; per term a, b.
+ *   data (complex), per problem: the left sets' blocks (set by set, i
+ *        ascending, column-major), the right sets' blocks, the terms' alphas.
+ * Returns the psi length, the algorithmic flops of one application (8 m n k
+ * per complex GEMM, both GEMMs of every (term, sector)) and the flops executed
+ * (each left product L_a[i] X_i is formed once and shared by its terms). */
+int tsc_blocksparse_set(tsc_ctx* ctx, int nproblems, const int* ints, long long nints, const double* data,
+                        long long ncplx, long long* dim, double* flops, double* exec_flops);
+/* Applies the batch on device pointers on the context stream, in TSC_FP64 or
+ * TSC_SPLIT_BF16 arithmetic (both sets of job lists are built by _set);
+ * tsc_hpsi_stats then reports its device time. */
+int tsc_blocksparse_apply(tsc_ctx* ctx, const void* d_in, void* d_out, int mode);
+
 /* H.psi on device pointers that allocates nothing (no counterpart in the
  * reference).  For callers that cannot call cudaMalloc or any allocating
  * library routine when they need H.psi (a host that owns the whole device

@@ -210,6 +210,18 @@ class Engine {
   void superblock_set(DModel&& sys, DModel&& env, Basis&& sys_bs, Basis&& env_bs, WLayout&& wl);
   void hpsi(const double2* d_in, double2* d_out);   // enqueue on st, in the context's precision
   void hpsi_form(const double2* d_in, double2* d_out, bool split);
+
+  // block-sparse batch (tsc_blocksparse_set/_apply, csrc/tsc_blocksparse.cu)
+  struct BlockSparse {
+    DevBufP ops, scratch;
+    TaskList p1, p2, p1s, p2s;
+    long long dim = 0;
+    double ref_flops = 0;
+    int nprob = 0;
+    bool valid = false;
+  } bs;
+  void blocksparse_set(int nprob, const int* ints, long long nints, const cplx* data, long long ncplx);
+  void blocksparse_apply(const double2* d_in, double2* d_out, bool split);
   // 0: complex FP64 throughout; 1: H.psi sector GEMMs as BF16 slices on the
   // tensor cores, Lanczos finished by FP64 iterations.  Applies from the next
   // superblock set on.

@@ -364,6 +364,7 @@ Engine::Engine(int Nx, int Ny, double t1, double t2, double J1, double J2, int d
 
 Engine::~Engine() {
   sb = Superblock();
+  bs = BlockSparse();
   sys_models.clear();
   env_models.clear();
   sys_truns.clear();

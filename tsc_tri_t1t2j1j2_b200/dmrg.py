@@ -111,6 +111,21 @@ class Context:
         superblock set."""
         self._check(self.L.tsc_set_precision(self.h, int(mode), float(split_tol)))
 
+    def blocksparse_set(self, problems):
+        """Block-sparse batch (tsc_blocksparse_set): `problems` is a list of
+        blocksparse.Problem; returns (psi length, algorithmic flops of one
+        application, flops executed)."""
+        from .blocksparse import pack
+        nprob, ints, data = pack(problems)
+        dim, flops, xflops = ctypes.c_longlong(), ctypes.c_double(), ctypes.c_double()
+        self._check(self.L.tsc_blocksparse_set(self.h, nprob, _iptr(ints), len(ints), _dptr(data), len(data),
+                                               ctypes.byref(dim), ctypes.byref(flops), ctypes.byref(xflops)))
+        return dim.value, flops.value, xflops.value
+
+    def blocksparse_apply(self, d_in: int, d_out: int, mode: int = 0):
+        """Applies the batch on device pointers (context stream)."""
+        self._check(self.L.tsc_blocksparse_apply(self.h, ctypes.c_void_p(d_in), ctypes.c_void_p(d_out), int(mode)))
+
     def hpsi_noalloc(self, d_in: int, d_out: int):
         """H.psi on device pointers that allocates nothing (scratch: a fixed 64 MiB
         device array shared by all calls; see include/tsc_gpu.h)."""
