@@ -339,6 +339,9 @@ def sweep_leg(dev):
         t0 = time.perf_counter()
         steps = ctx.get_ground_state(**SWEEP_CONFIG)
         wall = time.perf_counter() - t0
+        t1 = time.perf_counter()
+        dens = ctx.measure_density()
+        meas_s = time.perf_counter() - t1
         ctx.close()
         sw = [s for s in steps if s["phase"] != 0]
         res[name] = {
@@ -352,7 +355,13 @@ def sweep_leg(dev):
             "split_iters": int(sum(s["split_iters"] for s in sw)),
             "final_e0": steps[-1]["e0"],
             "min_e0": min(s["e0"] for s in steps),
+            "density_seconds": meas_s,
+            "density": dens,
         }
+    res["density_max_abs_diff_split_vs_fp64"] = float(np.max(np.abs(res["split"]["density"] - res["fp64"]["density"])))
+    res["density_sum_fp64"] = float(res["fp64"]["density"].sum())
+    for name in ("fp64", "split"):
+        del res[name]["density"]
     res["final_dE_over_E_split_vs_fp64"] = abs(res["split"]["final_e0"] - res["fp64"]["final_e0"]) / abs(
         res["fp64"]["final_e0"])
     res["sweep_speedup_split_over_fp64"] = res["fp64"]["sweep_seconds"] / res["split"]["sweep_seconds"]
@@ -369,12 +378,14 @@ def config1_leg(dev, with_cpu):
     with the CPU leg, the oracle (CPU restatement, OpenBLAS on all host cores)."""
     from tsc_tri_t1t2j1j2_b200 import Context
     res = {"workload": "YC4x6 t1=1 J1=0.4 t2=J2=0, warm-up m=100, 4 sweeps m=100,200,300,400, lanzero 1e-10"}
+    dens = {}
     for name, mode in (("fp64", Context.FP64), ("split", Context.SPLIT_BF16)):
         ctx = Context(device=dev.index, **CONFIG1)
         ctx.set_precision(mode, 1e-11)
         t0 = time.perf_counter()
         steps = ctx.get_ground_state(**CONFIG1_RUN)
         res[name] = {"seconds": time.perf_counter() - t0, "steps": len(steps), "final_e0": steps[-1]["e0"]}
+        dens[name] = ctx.measure_density()
         ctx.close()
     if with_cpu:
         sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -382,11 +393,16 @@ def config1_leg(dev, with_cpu):
         cfg = orc.RunConfig(Nx=6, Ny=4, t1=1.0, t2=0.0, J1=0.4, J2=0.0, kept_min=100, kept_warm=100,
                             sweeps=[100, 200, 300, 400], lanzero=1e-10)
         t0 = time.perf_counter()
-        ref = orc.Oracle(cfg).run()
+        o = orc.Oracle(cfg)
+        ref = o.run()
         sec = time.perf_counter() - t0
+        dref = o.measure_density()
         res["cpu_oracle"] = {"seconds": sec, "cores": os.cpu_count(), "steps": len(ref), "final_e0": ref[-1]["e0"]}
         res["fp64_final_dE_over_E_vs_oracle"] = abs(res["fp64"]["final_e0"] - ref[-1]["e0"]) / abs(ref[-1]["e0"])
         res["speedup_fp64_gpu_over_cpu"] = sec / res["fp64"]["seconds"]
+        res["density_max_abs_diff_fp64_vs_oracle"] = float(np.max(np.abs(dens["fp64"] - dref)))
+        res["density_max_abs_diff_split_vs_oracle"] = float(np.max(np.abs(dens["split"] - dref)))
+        res["split_final_dE_over_E_vs_oracle"] = abs(res["split"]["final_e0"] - ref[-1]["e0"]) / abs(ref[-1]["e0"])
     return res
 
 

@@ -141,6 +141,14 @@ int tsc_wave_transform(tsc_ctx* ctx, int dir, const int* ints, long long nints, 
  * Writes up to max_steps records; returns the number of Lanczos solves. */
 int tsc_dmrg_run(tsc_ctx* ctx, const tsc_sweep_config* sweep, tsc_step_log* log, int max_steps);
 
+/* <n_i> of every site in the last ground state of tsc_dmrg_run, sites 1..Nx*Ny
+ * in the lattice order (measure_operator_dia with num_elec, measure.f90:3-62,
+ * main.f90:268): the site operator is carried into the system / environment
+ * block through the run's stored bases and truncations (Get_sys_oper_dia,
+ * get_sys.f90:1147-1277) and measured on the last wavefunction.  Writes nsites
+ * >= Nx*Ny values; returns the number written. */
+int tsc_measure_density(tsc_ctx* ctx, double* out, int nsites);
+
 /* Serialises the superblock of the most recent step of tsc_dmrg_run whose
  * global solve index equals capture_step (set before the run with
  * tsc_set_capture); layout = tsc_superblock_set input with psi data. */

@@ -137,6 +137,13 @@ class Oracle {
   explicit Oracle(const Config& cfg);
   // Get_Ground_State (main.f90:114-209) with the configured schedule.
   void run(std::vector<StepLog>* log);
+  // measure_operator_dia with num_elec (measure.f90:3-62, called at main.f90:268):
+  // <n_i> of every site in the last ground state of run(), site order 1..Num_site.
+  std::vector<double> measure_density();
+  // Get_sys_oper_dia / Get_env_oper_dia (get_sys.f90:1147-1277), trun_idx = 1
+  // (main.f90:89), Truns = .true.: site operator `st` of site old_idx carried
+  // into the (truncated) block of length new_idx.
+  Block oper_dia_in_block(const Block& st, int old_idx, int new_idx, bool sys);
 
   // hot-path entry points restated (used directly by parity tests)
   void model_wave(Model& sys, Model& env, const Basis& sys_bs, const Basis& env_bs,

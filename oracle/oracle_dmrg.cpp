@@ -1034,4 +1034,112 @@ void Oracle::hamiltonian_env(Model& pre, const Basis& basis, const Block& trun) 
   pre.len = next.len;
 }
 
+// ---- measurement of <n_i> (measure.f90) ------------------------------------------
+
+Block Oracle::oper_dia_in_block(const Block& st, int old_idx, int new_idx, bool sys) {
+  const auto& bsm = sys ? sys_bsm : env_bsm;
+  const auto& truns = sys ? sys_truns : env_truns;
+  const int trun_idx = 1;
+  const int one = std::min(old_idx, new_idx), two = std::max(old_idx, new_idx);
+  Block cur, mid, out;
+  if (one <= two - 1) {
+    if (one <= 1) {
+      cur = st;
+    } else if (one <= trun_idx) {
+      update_site_dia(st, bsm.at(one), cur);
+    } else {
+      update_site_dia(st, bsm.at(one), mid);
+      update_trun_dia(mid, cur, truns.at(one));
+    }
+    int idx = one;
+    while (idx + 1 <= two - 1) {
+      update_block_dia(cur, bsm.at(idx + 1), mid);
+      idx++;
+      if (idx <= trun_idx) cur = mid;
+      else update_trun_dia(mid, cur, truns.at(idx));
+    }
+    update_block_dia(cur, bsm.at(idx + 1), out);
+  } else {
+    if (one <= 1) out = st;
+    else update_site_dia(st, bsm.at(two), out);
+  }
+  auto it = truns.find(two);
+  if (it == truns.end()) return out;   // lengths below trun_idx+1 carry no truncation
+  Block t;
+  update_trun_dia(out, t, it->second);
+  return t;
+}
+
+// measure_sys_block / measure_env_block (measure.f90:778-840, 905-970)
+static cplx measure_block(const Block& bl, const Basis& bs, const Wave& w, bool sys) {
+  cplx value = 0.0;
+  std::vector<cplx> mid;
+  for (const auto& ws : w.sub) {
+    const int qup = sys ? ws.sys_num_up : ws.env_num_up, qdn = sys ? ws.sys_num_down : ws.env_num_down;
+    for (const auto& S : bs.sub) {
+      if (S.new_num_up != qup || S.new_num_down != qdn) continue;
+      for (const auto& p : S.sub) {
+        const int y = find_blk(bl, p.bl_num_up, p.bl_num_down);
+        if (y < 0) continue;
+        const cplx coef = 1.0 / std::sqrt(1.0 + p.bl_num_down);
+        if (sys) {
+          mid.assign((size_t)p.sdim * ws.env_dim, 0.0);
+          zgemm('N', 'N', p.sdim, ws.env_dim, p.sdim, coef, bl.sub[y].mat.data(), p.sdim,
+                ws.vec.data() + p.spos, ws.sys_dim, czero, mid.data(), p.sdim);
+          for (int z = 0; z < ws.env_dim; ++z)
+            for (int r = 0; r < p.sdim; ++r)
+              value += std::conj(ws.vec[(size_t)z * ws.sys_dim + p.spos + r]) * mid[(size_t)z * p.sdim + r];
+        } else {
+          mid.assign((size_t)ws.sys_dim * p.sdim, 0.0);
+          zgemm('N', 'N', ws.sys_dim, p.sdim, p.sdim, coef, ws.vec.data() + (size_t)p.spos * ws.sys_dim,
+                ws.sys_dim, bl.sub[y].mat.data(), p.sdim, czero, mid.data(), ws.sys_dim);
+          for (int z = 0; z < p.sdim; ++z)
+            for (int r = 0; r < ws.sys_dim; ++r)
+              value += std::conj(mid[(size_t)z * ws.sys_dim + r]) * ws.vec[(size_t)(p.spos + z) * ws.sys_dim + r];
+        }
+      }
+    }
+  }
+  return value;
+}
+
+// measure_sys_site / measure_env_site (measure.f90:842-903, 971-1030)
+static cplx measure_site(const Block& st, const Basis& bs, const Wave& w, bool sys) {
+  cplx value = 0.0;
+  for (const auto& ws : w.sub) {
+    const int qup = sys ? ws.sys_num_up : ws.env_num_up, qdn = sys ? ws.sys_num_down : ws.env_num_down;
+    for (const auto& S : bs.sub) {
+      if (S.new_num_up != qup || S.new_num_down != qdn) continue;
+      for (const auto& p : S.sub) {
+        const int y = find_blk(st, p.st_num_up, p.st_num_down);
+        if (y < 0) continue;
+        const cplx coef = 1.0 / std::sqrt(1.0 + p.st_num_down);
+        cplx yita = 0.0;
+        if (sys) {
+          for (int z = 0; z < ws.env_dim; ++z)
+            for (int r = 0; r < p.sdim; ++r) yita += std::norm(ws.vec[(size_t)z * ws.sys_dim + p.spos + r]);
+        } else {
+          for (int z = 0; z < p.sdim; ++z)
+            for (int r = 0; r < ws.sys_dim; ++r) yita += std::norm(ws.vec[(size_t)(p.spos + z) * ws.sys_dim + r]);
+        }
+        value += yita * st.sub[y].mat[0] * coef;
+      }
+    }
+  }
+  return value;
+}
+
+std::vector<double> Oracle::measure_density() {
+  const Wave& w = disk_wave;
+  const int N = L.num_site, sl = w.sys_len, el = w.env_len;
+  std::vector<double> ave(N, 0.0);
+  for (int i = 1; i <= sl - 1; ++i)
+    ave[i - 1] = measure_block(oper_dia_in_block(num_elec, i, sl - 1, true), sys_bsm.at(sl), w, true).real();
+  ave[sl - 1] = measure_site(num_elec, sys_bsm.at(sl), w, true).real();
+  for (int i = 1; i <= el - 1; ++i)
+    ave[N - i] = measure_block(oper_dia_in_block(num_elec, i, el - 1, false), env_bsm.at(el), w, false).real();
+  ave[N - el] = measure_site(num_elec, env_bsm.at(el), w, false).real();
+  return ave;
+}
+
 }  // namespace orc

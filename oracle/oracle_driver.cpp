@@ -539,6 +539,20 @@ int orc_run(void* hp) {
 
 int orc_tot_num_up(void* hp) { return ((OrcHandle*)hp)->o->tot_num_up; }
 
+// <n_i> of the last ground state (measure_operator_dia); writes num_site values
+int orc_measure_density(void* hp, double* out) {
+  OrcHandle* h = (OrcHandle*)hp;
+  if (!h->o) return -1;
+  try {
+    std::vector<double> d = h->o->measure_density();
+    std::copy(d.begin(), d.end(), out);
+    return (int)d.size();
+  } catch (std::exception& e) {
+    h->err = e.what();
+    return -1;
+  }
+}
+
 // 12 doubles per step: phase, sys_len, env_len, e0, iters, num_state, trun_err,
 // entropy, entropy_mult, hpsi_calls, hpsi_seconds, hpsi_flops
 int orc_steps(void* hp, double* out) {

@@ -51,6 +51,8 @@ def lib():
         L.orc_hpsi_flat.argtypes = [vp, i, i, ctypes.POINTER(i), ctypes.POINTER(d), ctypes.POINTER(d), i,
                                     ctypes.POINTER(d), ctypes.POINTER(d)]
         L.orc_hpsi_flat.restype = i
+        L.orc_measure_density.argtypes = [vp, ctypes.POINTER(d)]
+        L.orc_measure_density.restype = i
         _lib = L
     return _lib
 
@@ -100,6 +102,15 @@ class Oracle:
         buf = np.zeros(12 * max(n, 1), dtype=np.float64)
         L.orc_steps(self.h, buf.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
         return [dict(zip(STEP_FIELDS, buf[12 * k:12 * k + 12].tolist())) for k in range(n)]
+
+    def measure_density(self):
+        """<n_i> of every site in the last ground state (measure_operator_dia)."""
+        L = lib()
+        out = np.zeros(self.cfg.Nx * self.cfg.Ny, dtype=np.float64)
+        n = L.orc_measure_density(self.h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+        if n < 0:
+            raise RuntimeError(L.orc_error(self.h).decode())
+        return out
 
     def capture(self):
         """Flat (ints, complex) serialisation of the captured superblock."""

@@ -135,8 +135,12 @@ def tj_ground_state(Nx, Ny, t1, t2, J1, J2, sign_t=-1.0, penalty=10.0):
     w, v = sla.eigsh(Hp, k=1, which="SA", tol=1e-13, maxiter=100000)
     e = float(w[0])
     s2 = float(np.real(v[:, 0].conj() @ (S2 @ v[:, 0])))
+    # site densities <n_q> of the ground state (site q+1 in the lattice numbering)
+    p = np.abs(v[:, 0]) ** 2
+    dens = [float(sum(p[k] for k, (um, dm) in enumerate(states) if ((um | dm) >> q) & 1)) for q in range(ns)]
     return {"Nx": Nx, "Ny": Ny, "t1": t1, "t2": t2, "J1": J1, "J2": J2, "n_sites": ns,
-            "n_electrons": ne, "dim": n, "e0_S0": e - penalty * s2, "S2": s2, "sign_t": sign_t}
+            "n_electrons": ne, "dim": n, "e0_S0": e - penalty * s2, "S2": s2, "sign_t": sign_t,
+            "density": dens}
 
 
 def main():

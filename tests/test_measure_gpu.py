@@ -1,0 +1,36 @@
+"""Site densities <n_i> measured on the device after a whole run
+(tsc_measure_density) against the oracle's measure_operator_dia.
+
+FP64 form at lanzero 1e-10, where the run follows the oracle's step by step:
+<= 1e-11 per site.  Split form at lanzero 1e-13 against the oracle at the same
+lanzero: <= 1e-7 per site (a density is first order in the difference of the
+two ground-state vectors, ~1e-8 measured).  Both sum to N_e to 1e-10."""
+import numpy as np
+import pytest
+
+import orc
+from tsc_tri_t1t2j1j2_b200 import Context
+
+RUN = dict(kept_min=60, kept_warm=60, sweeps=[60, 80])
+
+
+def oracle_density(lanzero):
+    cfg = orc.RunConfig(Nx=4, Ny=4, t1=1.0, t2=0.3, J1=0.4, J2=0.036, lanzero=lanzero, **RUN)
+    o = orc.Oracle(cfg)
+    o.run()
+    return o.measure_density()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("mode,lanzero,tol", [(Context.FP64, 1e-10, 1e-11), (Context.SPLIT_BF16, 1e-13, 1e-7)])
+def test_density_matches_oracle(mode, lanzero, tol):
+    ref = oracle_density(lanzero)
+    ctx = Context(4, 4, 1.0, 0.3, 0.4, 0.036)
+    try:
+        ctx.set_precision(mode, 1e-11)
+        ctx.get_ground_state(lanzero=lanzero, **RUN)
+        dens = ctx.measure_density()
+    finally:
+        ctx.close()
+    assert np.max(np.abs(dens - ref)) <= tol
+    assert abs(dens.sum() - round(ref.sum())) <= 1e-10

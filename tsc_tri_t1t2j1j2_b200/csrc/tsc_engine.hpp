@@ -222,6 +222,15 @@ class Engine {
   } bs;
   void blocksparse_set(int nprob, const int* ints, long long nints, const cplx* data, long long ncplx);
   void blocksparse_apply(const double2* d_in, double2* d_out, bool split);
+
+  // measurement of the last ground state (csrc/tsc_measure.cu, measure.f90)
+  std::vector<double> measure_density();
+  DBlock oper_dia_in_block(const SiteOp& so, int old_idx, int new_idx, bool sys);
+  DBlock site_as_block(const SiteOp& so);
+  DBlock site_dia(const SiteOp& so, const Basis& basis);
+  DBlock block_dia(const DBlock& blk, const Basis& basis);
+  DBlock trun_dia(const DBlock& ori, const DBlock& trun);
+  double expect_dia(const DBlock* bl, const SiteOp* so, const Basis& bs, bool sys);
   // 0: complex FP64 throughout; 1: H.psi sector GEMMs as BF16 slices on the
   // tensor cores, Lanczos finished by FP64 iterations.  Applies from the next
   // superblock set on.

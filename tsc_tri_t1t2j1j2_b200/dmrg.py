@@ -210,6 +210,13 @@ class Context:
             out.append({f: getattr(s, f) for f, _ in _lib.StepLog._fields_})
         return out
 
+    def measure_density(self):
+        """<n_i> of every site in the last ground state of get_ground_state
+        (measure_operator_dia, measure.f90:3-62)."""
+        out = np.zeros(self.Nx * self.Ny, dtype=np.float64)
+        self._check(self.L.tsc_measure_density(self.h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), len(out)))
+        return out
+
     def capture(self):
         ti, tn, td, tc = P(ctypes.c_int)(), ctypes.c_longlong(), P(ctypes.c_double)(), ctypes.c_longlong()
         sl, el = ctypes.c_int(), ctypes.c_int()
