@@ -457,6 +457,28 @@ def config5_leg(torch, dev, zgemm_peak):
     return out
 
 
+def points_leg(dev):
+    """Eight parameter points of the reference's CPU-runnable case (YC4x6, 4 sweeps
+    m=100..400), t2 = 0, 0.05, ..., 0.35 with J2 = J1 (t2/t1)^2: run one after the
+    other, then all at once (run_parameter_points: a context and host thread per
+    point).  Seconds of both and the final energies' largest difference."""
+    from tsc_tri_t1t2j1j2_b200 import Context, run_parameter_points
+    pts = [dict(Nx=6, Ny=4, t1=1.0, t2=0.05 * k, J1=0.4, J2=0.4 * (0.05 * k) ** 2) for k in range(8)]
+    t0 = time.perf_counter()
+    seq = []
+    for p in pts:
+        ctx = Context(device=dev.index, **p)
+        seq.append(ctx.get_ground_state(**CONFIG1_RUN)[-1]["e0"])
+        ctx.close()
+    t_seq = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    par = [st[-1]["e0"] for st in run_parameter_points(pts, CONFIG1_RUN, device=dev.index)]
+    t_par = time.perf_counter() - t0
+    return {"workload": "8 x YC4x6 (t2 = 0..0.35, J2 = J1 t2^2), 4 sweeps m=100..400, lanzero 1e-10",
+            "sequential_seconds": t_seq, "concurrent_seconds": t_par, "throughput_gain": t_seq / t_par,
+            "final_e0_max_rel_diff": max(abs(a - b) / abs(b) for a, b in zip(par, seq))}
+
+
 def run_gpu(args):
     import torch
     from tsc_tri_t1t2j1j2_b200 import Context
@@ -553,6 +575,7 @@ def run_gpu(args):
         if not args.no_sweep:
             line["sweep"] = sweep_leg(dev)
             line["sweep_config1"] = config1_leg(dev, ws == 1 and not args.no_cpu)
+            line["parameter_points"] = points_leg(dev)
         if ws == 1 and not args.no_cpu:
             cpu_out, sec, flops, wall = cpu_hpsi(sb, 1)
             err = float(np.max(np.abs(gpu_out - cpu_out)) / np.max(np.abs(cpu_out)))

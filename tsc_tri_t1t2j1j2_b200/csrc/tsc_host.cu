@@ -1,6 +1,7 @@
 // Host set-up of the engine: device memory, lattice tables, SU(2) 6j symbols,
 // site operators, bases and task-list packing.
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -168,17 +169,20 @@ DevBuf::~DevBuf() {
 // ---- SU(2) coefficients --------------------------------------------------------
 // Racah's closed form for the 6j symbol with doubled arguments (the reference's
 // W6JS, block.f90:3744-3795, evaluates the same sum with a table of factorials).
-static double g_fact[171];
-static bool g_fact_ready = false;
-static void fact_init() {
-  if (g_fact_ready) return;
-  g_fact[0] = 1.0;
-  for (int i = 1; i <= 170; ++i) g_fact[i] = g_fact[i - 1] * (double)(float)i;
-  g_fact_ready = true;
+// factorials as FACTRL builds them (block.f90:3688-3696); initialised once,
+// thread-safely, by the first caller of any engine
+static const double* factorials() {
+  static const std::array<double, 171> f = [] {
+    std::array<double, 171> a{};
+    a[0] = 1.0;
+    for (int i = 1; i <= 170; ++i) a[i] = a[i - 1] * (double)(float)i;
+    return a;
+  }();
+  return f.data();
 }
 
 double w6j(int j1, int j2, int j3, int l1, int l2, int l3) {
-  fact_init();
+  const double* g_fact = factorials();
   // triangle (j1 j2 j3), (j1 l2 l3), (l1 j2 l3), (l1 l2 j3) with integer sums
   auto tri = [](int a, int b, int c) { return c <= a + b && c >= std::abs(a - b) && ((a + b + c) & 1) == 0; };
   if (!tri(j1, j2, j3) || !tri(j1, l2, l3) || !tri(l1, j2, l3) || !tri(l1, l2, j3)) return 0.0;
@@ -193,7 +197,7 @@ double w6j(int j1, int j2, int j3, int l1, int l2, int l3) {
     if (w % 4 != 0) den = -den;
     omega = omega + g_fact[w / 2 + 1] / den;
   }
-  auto delta = [](int a, int b, int c) {
+  auto delta = [g_fact](int a, int b, int c) {
     return g_fact[(a + b - c) / 2] * g_fact[(a - b + c) / 2] * g_fact[(-a + b + c) / 2] / g_fact[(a + b + c) / 2 + 1];
   };
   double th = delta(j1, j2, j3) * delta(j1, l2, l3) * delta(l1, j2, l3) * delta(l1, l2, j3);

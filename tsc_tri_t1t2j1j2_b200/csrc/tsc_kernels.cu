@@ -595,13 +595,9 @@ template <int TM, int TN, int MINB>
 cudaError_t launch_tile(const GJob* jobs, int njobs, const GGroup* groups, const GTerm* terms, Bases bases,
                         cudaStream_t st) {
   const size_t smem = sizeof(SmemTiles<TM, TN>);
-  static bool attr = false;
-  if (!attr) {
-    cudaError_t e = cudaFuncSetAttribute(grouped_zgemm_kernel<TM, TN, MINB>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-    attr = true;
-  }
+  static std::atomic<unsigned long long> attr{0};
+  cudaError_t e = ensure_smem_attr(grouped_zgemm_kernel<TM, TN, MINB>, (int)smem, attr);
+  if (e != cudaSuccess) return e;
   grouped_zgemm_kernel<TM, TN, MINB><<<njobs, GEMM_THREADS, smem, st>>>(jobs, groups, terms, bases);
   return cudaGetLastError();
 }

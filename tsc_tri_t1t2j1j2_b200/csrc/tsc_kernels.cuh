@@ -1,5 +1,6 @@
 // Device task formats shared by the host task builders and the kernels.
 #pragma once
+#include <atomic>
 #include <cuda_runtime.h>
 #include <cstdint>
 
@@ -67,6 +68,21 @@ cudaError_t launch_grouped_zgemm_split(const GJob* jobs, int njobs, const GGroup
 // bounded mbarrier waits runs out.
 cudaError_t split_fault_flag(int* host_flag, int clear);
 constexpr int SPLIT_TILE_M = 128, SPLIT_TILE_N = 64;
+
+// Sets a kernel's dynamic shared-memory limit once per device (the attribute
+// belongs to the current device's context; concurrent first calls set the same
+// value).  `done` is the kernel's own bitmask of devices already set.
+template <class K>
+cudaError_t ensure_smem_attr(K kernel, int bytes, std::atomic<unsigned long long>& done) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  const unsigned long long bit = 1ull << (dev & 63);
+  if (done.load(std::memory_order_acquire) & bit) return cudaSuccess;
+  e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e == cudaSuccess) done.fetch_or(bit, std::memory_order_acq_rel);
+  return e;
+}
 cudaError_t launch_reduce_partials(const GReduce* reds, int nred, const GGroup* groups, Bases bases,
                                    long long max_elems, cudaStream_t st);
 

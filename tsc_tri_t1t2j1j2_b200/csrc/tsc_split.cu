@@ -513,20 +513,13 @@ grouped_zgemm_split_kernel(const GJob* __restrict__ jobs, int njobs, const GGrou
 cudaError_t launch_grouped_zgemm_split(const GJob* jobs, int njobs, const GGroup* groups, const GTerm* terms,
                                        Bases bases, cudaStream_t st) {
   if (njobs <= 0) return cudaSuccess;
-  static bool attr_set = false;
-  if (!attr_set) {
-    cudaError_t e = cudaFuncSetAttribute(grouped_zgemm_split_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         SMEM_BYTES);
-    if (e != cudaSuccess) return e;
-    attr_set = true;
-  }
-  static int nsm = 0;
-  if (!nsm) {
-    int dev = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    if (nsm <= 0) nsm = 148;
-  }
+  static std::atomic<unsigned long long> attr{0};
+  cudaError_t e = ensure_smem_attr(grouped_zgemm_split_kernel, SMEM_BYTES, attr);
+  if (e != cudaSuccess) return e;
+  int dev = 0, nsm = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  if (nsm <= 0) nsm = 148;
   const int grid = njobs < nsm ? njobs : nsm;
   grouped_zgemm_split_kernel<<<grid, SP_THREADS, SMEM_BYTES, st>>>(jobs, njobs, groups, terms, bases);
   return cudaGetLastError();

@@ -225,3 +225,26 @@ class Context:
         ints = np.ctypeslib.as_array(ti, shape=(tn.value,)).copy()
         data = np.ctypeslib.as_array(td, shape=(2 * tc.value,)).copy().view(np.complex128)
         return ints, data, sl.value, el.value
+
+
+def run_parameter_points(points, sweep, precision=0, device=0, workers=None, measure=False):
+    """Independent ground-state searches, one per model-parameter dict of
+    `points` (keyword arguments of Context), on one GPU at the same time.  Small
+    systems leave most of the GPU idle; each point gets its own context (stream,
+    device-memory arena, eigensolver lanes) driven from its own host thread, so
+    their kernels interleave on the device.  `sweep` holds the keyword arguments
+    of get_ground_state.  Returns, per point, the step records (and the site
+    densities when `measure` is set)."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    def one(p):
+        ctx = Context(device=device, **p)
+        try:
+            ctx.set_precision(precision)
+            steps = ctx.get_ground_state(**sweep)
+            return (steps, ctx.measure_density()) if measure else steps
+        finally:
+            ctx.close()
+
+    with ThreadPoolExecutor(max_workers=workers or len(points)) as ex:
+        return list(ex.map(one, points))
