@@ -342,6 +342,7 @@ def sweep_leg(dev):
         t1 = time.perf_counter()
         dens = ctx.measure_density()
         meas_s = time.perf_counter() - t1
+        tuned = ctx.autotune_table()
         ctx.close()
         sw = [s for s in steps if s["phase"] != 0]
         res[name] = {
@@ -357,6 +358,7 @@ def sweep_leg(dev):
             "min_e0": min(s["e0"] for s in steps),
             "density_seconds": meas_s,
             "density": dens,
+            "autotune_ms_per_gflop": {str(k): v for k, v in tuned.items()},
         }
     res["density_max_abs_diff_split_vs_fp64"] = float(np.max(np.abs(res["split"]["density"] - res["fp64"]["density"])))
     res["density_sum_fp64"] = float(res["fp64"]["density"].sum())

@@ -390,3 +390,25 @@ int tsc_set_precision(tsc_ctx* ctx, int mode, double split_tol) {
     if (split_tol > 0) ctx->eng->split_tol_ = split_tol;
   });
 }
+
+int tsc_set_autotune(tsc_ctx* ctx, int on) {
+  return guard(ctx, [&] {
+    if (!ctx->eng) throw Error(TSC_E_STATE, "no engine");
+    ctx->eng->autotune_ = on != 0;
+  });
+}
+
+int tsc_autotune_table(tsc_ctx* ctx, int* cls, double* ms_per_gflop, int max_classes) {
+  int n = 0;
+  int rc = guard(ctx, [&] {
+    if (!ctx->eng) throw Error(TSC_E_STATE, "no engine");
+    for (const auto& kv : ctx->eng->tune_ms_) {
+      if (n < max_classes && cls && ms_per_gflop) {
+        cls[n] = kv.first;
+        for (int c = 0; c < Engine::kTuneCands; ++c) ms_per_gflop[4 * n + c] = kv.second[c];
+      }
+      n++;
+    }
+  });
+  return rc < 0 ? rc : n;
+}

@@ -252,6 +252,7 @@ void Engine::lanczos_run(double2* d_psi, double lanzero, double rel_tol, bool sp
   auto read_back = [&](int slot, int count) {
     cuda_check(cudaMemcpyAsync(h_scal + slot, d_scal + slot, count * sizeof(double), cudaMemcpyDeviceToHost, st), "d2h");
     cuda_check(cudaStreamSynchronize(st), "sync");
+    tune_observe();
   };
   // lowest eigenpair of T_m (alpha_1..m, beta_1..m-1) from the device slots
   auto tridiag_vec = [&](int m) {

@@ -165,7 +165,7 @@ struct TaskList {
   // Packs the lists for the device.  Groups whose term list is much longer than
   // total_cost / (slots * waves) are split into contiguous term chunks, each
   // computing a partial tile; a fixed-order reduction then writes the group.
-  void upload(cudaStream_t st, int slots = 296, int waves = 4);
+  void upload(cudaStream_t st, int slots = 296, int waves = 4, int tile_override = 0);
   // The same lists for the split-precision kernel (the host lists are kept).
   void upload_split(cudaStream_t st);
 };
@@ -201,6 +201,10 @@ class Engine {
     TaskList merge;            // hmerge axpy tasks
     TaskList p1, p2;           // H.psi phase 1 (intermediates) and phase 2 (outputs)
     TaskList p1s, p2s;         // the same, tiled for the split-precision kernel
+    TaskList q1, q2;           // a candidate schedule being timed by the autotuner
+    int tune_class = -1;       // size class of this superblock (-1: not tuned)
+    int tune_cand = -1;        // candidate in q1/q2, used by the next H.psi
+    bool tune_pending = false; // that H.psi ran and its time is still to be read
     long long scratch_elems = 0;
     DevBufP scratch;
     double ref_flops = 0;      // algorithmic flops of one model_wave (reference order)
@@ -238,6 +242,23 @@ class Engine {
   double split_tol_ = 1e-9;   // relative Ritz-value change that ends the split iterations
   bool split_now_ = false;    // the current superblock's solve uses the split form
   bool in_warmup_ = false;    // set while the warm-up (infinite-lattice) steps run
+
+  // Autotuner of the FP64 H.psi schedule: for each size class (log2 of the
+  // H.psi GFLOP, superblocks of >= 8 GFLOP) the candidate (tile edge, waves)
+  // schedules are timed, one per superblock on its first H.psi, in device
+  // milliseconds per algorithmic GFLOP; once all are timed the class keeps the
+  // fastest.  tsc_set_autotune switches it off (schedule fixed, results
+  // bit-reproducible run to run).
+  struct TuneCand {
+    int tile, waves;
+  };
+  static constexpr int kTuneCands = 4;
+  const TuneCand tune_cands_[kTuneCands] = {{32, 4}, {32, 2}, {32, 8}, {64, 4}};
+  std::map<int, std::array<double, kTuneCands>> tune_ms_;   // class -> ms/GFLOP (<0: not timed)
+  bool autotune_ = true;
+  cudaEvent_t tune_ev_[2] = {nullptr, nullptr};   // bracket the candidate's H.psi
+  void tune_setup();          // called by build_hpsi_tasks once p1/p2 are built
+  void tune_observe();        // after a synchronisation: records a pending timing
   Stats last_stats;
 
   // Lanczos (eigen.f90:4-199) on the current superblock; psi device buffer in/out

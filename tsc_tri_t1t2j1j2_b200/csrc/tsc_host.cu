@@ -386,6 +386,8 @@ Engine::~Engine() {
   if (ev0) cudaEventDestroy(ev0);
   if (ev1) cudaEventDestroy(ev1);
   for (cudaEvent_t e : hpsi_events) cudaEventDestroy(e);
+  for (cudaEvent_t e : tune_ev_)
+    if (e) cudaEventDestroy(e);
   if (st) cudaStreamDestroy(st);
 }
 
@@ -517,8 +519,8 @@ void TaskList::upload_split(cudaStream_t st) {
   upload(st, 148 * 2, 4);
 }
 
-void TaskList::upload(cudaStream_t st, int slots, int waves) {
-  tile = default_tile();
+void TaskList::upload(cudaStream_t st, int slots, int waves, int tile_override) {
+  tile = tile_override ? tile_override : default_tile();
   int TMt = tile, TNt = tile;
   if (split) {
     TMt = SPLIT_TILE_M;

@@ -982,14 +982,73 @@ void Engine::build_hpsi_tasks() {
     S.p1s.gterms.clear();
     S.p2s.gterms.clear();
   }
-  S.p1.upload(st);
-  S.p2.upload(st);
+  tune_setup();
   S.p1.gterms.clear();
   S.p2.gterms.clear();
+  S.q1.gterms.clear();
+  S.q2.gterms.clear();
   S.scratch = std::make_shared<DevBuf>((size_t)std::max<long long>(B.scr, 1), st, false);
 }
 
+void Engine::tune_setup() {
+  Superblock& S = sb;
+  const double gflop = S.ref_flops / 1e9;
+  S.tune_class = (autotune_ && gflop >= 8.0) ? (int)std::floor(std::log2(gflop)) : -1;
+  S.tune_cand = -1;
+  S.tune_pending = false;
+  if (S.tune_class < 0) {
+    S.p1.upload(st);
+    S.p2.upload(st);
+    return;
+  }
+  auto it = tune_ms_.find(S.tune_class);
+  if (it == tune_ms_.end()) {
+    std::array<double, kTuneCands> none;
+    none.fill(-1.0);
+    it = tune_ms_.emplace(S.tune_class, none).first;
+  }
+  const auto& ms = it->second;
+  int best = 0, next = -1;
+  for (int c = 0; c < kTuneCands; ++c) {
+    if (ms[c] < 0 && next < 0) next = c;
+    if (ms[c] >= 0 && (ms[best] < 0 || ms[c] < ms[best])) best = c;
+  }
+  if (next < 0) {   // class tuned: its fastest schedule only
+    S.p1.upload(st, 296, tune_cands_[best].waves, tune_cands_[best].tile);
+    S.p2.upload(st, 296, tune_cands_[best].waves, tune_cands_[best].tile);
+    return;
+  }
+  // the class's best so far (or the default) for the solve, the next untimed
+  // candidate for its first H.psi
+  const TuneCand base = ms[best] >= 0 ? tune_cands_[best] : tune_cands_[0];
+  S.q1.groups = S.p1.groups;
+  S.q1.gterms = S.p1.gterms;
+  S.q2.groups = S.p2.groups;
+  S.q2.gterms = S.p2.gterms;
+  S.p1.upload(st, 296, base.waves, base.tile);
+  S.p2.upload(st, 296, base.waves, base.tile);
+  S.q1.upload(st, 296, tune_cands_[next].waves, tune_cands_[next].tile);
+  S.q2.upload(st, 296, tune_cands_[next].waves, tune_cands_[next].tile);
+  S.tune_cand = next;
+}
+
+void Engine::tune_observe() {
+  Superblock& S = sb;
+  if (!S.tune_pending || cudaEventQuery(tune_ev_[1]) != cudaSuccess) return;
+  S.tune_pending = false;
+  float ms = 0.f;
+  if (cudaEventElapsedTime(&ms, tune_ev_[0], tune_ev_[1]) != cudaSuccess) return;
+  tune_ms_[S.tune_class][S.tune_cand] = ms / (S.ref_flops / 1e9);
+  S.tune_cand = -1;
+  S.q1 = TaskList();
+  S.q2 = TaskList();
+}
+
 void Engine::superblock_set(DModel&& sys, DModel&& env, Basis&& sys_bs, Basis&& env_bs, WLayout&& wl) {
+  if (sb.valid && sb.tune_pending) {   // a candidate timed on the previous superblock is read first
+    cudaEventSynchronize(tune_ev_[1]);
+    tune_observe();
+  }
   sb = Superblock();
   sb.sys = std::move(sys);
   sb.env = std::move(env);
@@ -1010,13 +1069,22 @@ void Engine::hpsi(const double2* d_in, double2* d_out) { hpsi_form(d_in, d_out, 
 
 void Engine::hpsi_form(const double2* d_in, double2* d_out, bool split) {
   if (!sb.valid) throw Error(-4, "no superblock");
-  TaskList& a = split ? sb.p1s : sb.p1;
-  TaskList& b = split ? sb.p2s : sb.p2;
+  // the autotuner's candidate runs the first FP64 H.psi after the superblock is set
+  const bool probe = !split && sb.tune_cand >= 0 && !sb.tune_pending;
+  TaskList& a = split ? sb.p1s : (probe ? sb.q1 : sb.p1);
+  TaskList& b = split ? sb.p2s : (probe ? sb.q2 : sb.p2);
   if (split && !a.split) throw Error(-4, "split-precision lists were not built for this superblock");
+  if (probe) {
+    sb.tune_pending = true;
+    for (auto& e : tune_ev_)
+      if (!e) cuda_check(cudaEventCreate(&e), "cudaEventCreate");
+    cuda_check(cudaEventRecord(tune_ev_[0], st), "event");
+  }
   cuda_check(cudaEventRecord(ev0, st), "event");
   run_tasks(a, const_cast<double2*>(d_in), d_out, sb.scratch->p);
   run_tasks(b, const_cast<double2*>(d_in), d_out, sb.scratch->p);
   cuda_check(cudaEventRecord(ev1, st), "event");
+  if (probe) cuda_check(cudaEventRecord(tune_ev_[1], st), "event");
   last_stats.launches = (a.njobs > 0) + (b.njobs > 0) + (a.nreds > 0) + (b.nreds > 0);
   last_stats.hpsi_flops = sb.ref_flops;
 }

@@ -126,6 +126,18 @@ class Context:
         """Applies the batch on device pointers (context stream)."""
         self._check(self.L.tsc_blocksparse_apply(self.h, ctypes.c_void_p(d_in), ctypes.c_void_p(d_out), int(mode)))
 
+    def set_autotune(self, on: bool):
+        """FP64 H.psi schedule autotuner (on by default; off = fixed schedule)."""
+        self._check(self.L.tsc_set_autotune(self.h, 1 if on else 0))
+
+    def autotune_table(self):
+        """{size class (floor log2 GFLOP): ms per GFLOP of the candidates
+        (tile 32 / 4 waves, 32 / 2, 32 / 8, 64 / 4), None where not timed}."""
+        cls = (ctypes.c_int * 64)()
+        ms = (ctypes.c_double * 256)()
+        n = self._check(self.L.tsc_autotune_table(self.h, cls, ms, 64))
+        return {cls[i]: [ms[4 * i + c] if ms[4 * i + c] >= 0 else None for c in range(4)] for i in range(min(n, 64))}
+
     def hpsi_noalloc(self, d_in: int, d_out: int):
         """H.psi on device pointers that allocates nothing (scratch: a fixed 64 MiB
         device array shared by all calls; see include/tsc_gpu.h)."""
