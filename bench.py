@@ -498,6 +498,8 @@ def run_gpu(args):
     ctx.set_superblock_flat(sl, el, ints, data)
     assert ctx.dim == n
     stream = torch.cuda.ExternalStream(ctx.stream, device=dev)
+    schedule = ctx.autotune_superblock(3)   # the autotuner's pick for this superblock, before timing
+    tune_table = ctx.autotune_table()
     psi = torch.from_numpy(data[off:off + n].copy()).to(dev)
     out = torch.empty_like(psi)
     torch.cuda.synchronize()
@@ -565,7 +567,9 @@ def run_gpu(args):
             "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                          "frac": achieved / peak, "traffic": TRAFFIC_BYTES_PER_STEP if args.scale == 1 else None,
                          "peak_source": "cuBLAS ZGEMM 4096^3 complex128 measured in this run (FP64 DMMA)",
-                         "kernel": "grouped_zgemm (2 launches per H.psi)"},
+                         "kernel": "grouped_zgemm (2 launches per H.psi)",
+                         "schedule": {"tile": schedule[0], "waves": schedule[1],
+                                      "candidates_ms_per_gflop": {str(k): v for k, v in tune_table.items()}}},
             "e2e": {"value": e2e, "unit": "TFLOP/s", "h2d_bytes_per_step": 16 * n, "d2h_bytes_per_step": 16 * n},
             "gpu_launches": 2 * args.steps,
             "clocks": clocks.summary(),

@@ -195,6 +195,10 @@ int tsc_set_autotune(tsc_ctx* ctx, int on);
  * (tile 32, 4 waves), (32, 2), (32, 8), (64, 4); negative = not timed yet.
  * Returns the number of classes. */
 int tsc_autotune_table(tsc_ctx* ctx, int* cls, double* ms_per_gflop, int max_classes);
+/* Times every candidate schedule on the current superblock now (best of reps
+ * FP64 H.psi each, on a scratch vector), records them for its size class and
+ * keeps the fastest for this superblock; returns that candidate's index. */
+int tsc_autotune_superblock(tsc_ctx* ctx, int reps);
 
 /* Block-sparse H.psi on a batch of independent problems, all of them in the
  * same two grouped launches (no counterpart in the reference, which applies

@@ -21,7 +21,7 @@ EXPORTED = [
     "tsc_renormalize", "tsc_wave_transform", "tsc_dmrg_run", "tsc_set_capture", "tsc_get_capture",
     "tsc_hpsi_stats", "tsc_stream", "tsc_hpsi_noalloc", "tsc_set_precision",
     "tsc_blocksparse_set", "tsc_blocksparse_apply", "tsc_measure_density", "tsc_set_autotune",
-    "tsc_autotune_table",
+    "tsc_autotune_table", "tsc_autotune_superblock",
 ]
 
 
@@ -93,6 +93,7 @@ def load():
     L.tsc_measure_density.argtypes = [c_void, ctypes.POINTER(c_double), c_int]
     L.tsc_set_autotune.argtypes = [c_void, c_int]
     L.tsc_autotune_table.argtypes = [c_void, ctypes.POINTER(c_int), ctypes.POINTER(c_double), c_int]
+    L.tsc_autotune_superblock.argtypes = [c_void, c_int]
     _lib = L
     return L
 

@@ -412,3 +412,12 @@ int tsc_autotune_table(tsc_ctx* ctx, int* cls, double* ms_per_gflop, int max_cla
   });
   return rc < 0 ? rc : n;
 }
+
+int tsc_autotune_superblock(tsc_ctx* ctx, int reps) {
+  int win = 0;
+  int rc = guard(ctx, [&] {
+    if (!ctx->eng || !ctx->eng->sb.valid) throw Error(TSC_E_STATE, "no superblock set");
+    win = ctx->eng->tune_superblock(reps);
+  });
+  return rc < 0 ? rc : win;
+}

@@ -259,6 +259,7 @@ class Engine {
   cudaEvent_t tune_ev_[2] = {nullptr, nullptr};   // bracket the candidate's H.psi
   void tune_setup();          // called by build_hpsi_tasks once p1/p2 are built
   void tune_observe();        // after a synchronisation: records a pending timing
+  int tune_superblock(int reps);   // times every candidate on the current superblock
   Stats last_stats;
 
   // Lanczos (eigen.f90:4-199) on the current superblock; psi device buffer in/out

@@ -10,6 +10,7 @@
 // -- the reuse the reference forgoes when it recomputes GEMM1 per task
 // (get_sys.f90:3384-3389).  Coefficients, signs and sector searches follow the
 // reference kernels (get_sys.f90:1783-5204) term by term.
+#include <algorithm>
 #include <cmath>
 #include <map>
 #include <tuple>
@@ -983,8 +984,6 @@ void Engine::build_hpsi_tasks() {
     S.p2s.gterms.clear();
   }
   tune_setup();
-  S.p1.gterms.clear();
-  S.p2.gterms.clear();
   S.q1.gterms.clear();
   S.q2.gterms.clear();
   S.scratch = std::make_shared<DevBuf>((size_t)std::max<long long>(B.scr, 1), st, false);
@@ -1030,6 +1029,49 @@ void Engine::tune_setup() {
   S.q1.upload(st, 296, tune_cands_[next].waves, tune_cands_[next].tile);
   S.q2.upload(st, 296, tune_cands_[next].waves, tune_cands_[next].tile);
   S.tune_cand = next;
+}
+
+// Times every candidate schedule on the current superblock (FP64 H.psi of a
+// scratch vector, best of `reps` device timings each), records them for its size
+// class and keeps the fastest for the superblock.  Returns that candidate.
+int Engine::tune_superblock(int reps) {
+  Superblock& S = sb;
+  if (!S.valid) throw Error(-4, "no superblock");
+  const long long n = S.wl.dim;
+  DevBuf x((size_t)std::max<long long>(n, 1), st, true), y((size_t)std::max<long long>(n, 1), st, false);
+  const int cls = (int)std::floor(std::log2(std::max(S.ref_flops / 1e9, 1e-9)));
+  std::array<double, kTuneCands> ms;
+  for (int c = 0; c < kTuneCands; ++c) {
+    TaskList a, b;
+    a.groups = S.p1.groups;
+    a.gterms = S.p1.gterms;
+    b.groups = S.p2.groups;
+    b.gterms = S.p2.gterms;
+    a.upload(st, 296, tune_cands_[c].waves, tune_cands_[c].tile);
+    b.upload(st, 296, tune_cands_[c].waves, tune_cands_[c].tile);
+    double best = 1e30;
+    for (int r = 0; r < std::max(reps, 1) + 1; ++r) {   // the first run warms up
+      cuda_check(cudaEventRecord(ev0, st), "event");
+      run_tasks(a, x.p, y.p, S.scratch->p);
+      run_tasks(b, x.p, y.p, S.scratch->p);
+      cuda_check(cudaEventRecord(ev1, st), "event");
+      cuda_check(cudaEventSynchronize(ev1), "sync");
+      float t = 0.f;
+      cuda_check(cudaEventElapsedTime(&t, ev0, ev1), "elapsed");
+      if (r > 0) best = std::min(best, (double)t);
+    }
+    ms[c] = best / (S.ref_flops / 1e9);
+  }
+  tune_ms_[cls] = ms;
+  const int win = (int)(std::min_element(ms.begin(), ms.end()) - ms.begin());
+  S.p1.upload(st, 296, tune_cands_[win].waves, tune_cands_[win].tile);
+  S.p2.upload(st, 296, tune_cands_[win].waves, tune_cands_[win].tile);
+  S.tune_cand = -1;
+  S.tune_pending = false;
+  S.q1 = TaskList();
+  S.q2 = TaskList();
+  cuda_check(cudaStreamSynchronize(st), "sync");
+  return win;
 }
 
 void Engine::tune_observe() {

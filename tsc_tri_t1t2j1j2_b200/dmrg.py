@@ -138,6 +138,13 @@ class Context:
         n = self._check(self.L.tsc_autotune_table(self.h, cls, ms, 64))
         return {cls[i]: [ms[4 * i + c] if ms[4 * i + c] >= 0 else None for c in range(4)] for i in range(min(n, 64))}
 
+    TUNE_CANDIDATES = ((32, 4), (32, 2), (32, 8), (64, 4))   # (CTA tile edge, waves)
+
+    def autotune_superblock(self, reps: int = 3):
+        """Times every candidate H.psi schedule on the current superblock and keeps
+        the fastest; returns its (tile edge, waves)."""
+        return self.TUNE_CANDIDATES[self._check(self.L.tsc_autotune_superblock(self.h, int(reps)))]
+
     def hpsi_noalloc(self, d_in: int, d_out: int):
         """H.psi on device pointers that allocates nothing (scratch: a fixed 64 MiB
         device array shared by all calls; see include/tsc_gpu.h)."""
