@@ -184,15 +184,16 @@ int tsc_set_precision(tsc_ctx* ctx, int mode, double split_tol);
 
 /* The FP64 H.psi schedule autotuner (on at creation; no counterpart in the
  * reference).  For superblocks of >= 8 GFLOP per H.psi it times candidate
- * schedules (CTA tile edge 32 or 64, long term lists split into chunks for 2, 4
- * or 8 waves of CTAs), one candidate on the first H.psi of each superblock of a
+ * schedules (CTA tile of output rows x columns, long term lists split into
+ * chunks for 4 or 8 waves of CTAs), one candidate on the first H.psi of each superblock of a
  * size class (log2 GFLOP), and keeps each class's fastest.  Results are the
  * same H.psi up to the summation order of split term lists; off (0) fixes the
  * schedule, so repeated runs are bit-identical. */
 int tsc_set_autotune(tsc_ctx* ctx, int on);
 /* The autotuner's measurements: for up to max_classes size classes, class[i]
  * (floor log2 of the H.psi GFLOP) and ms_per_gflop[4*i + c] for candidate c =
- * (tile 32, 4 waves), (32, 2), (32, 8), (64, 4); negative = not timed yet.
+ * (tile 32x32, 4 waves), (32x32, 8), (64x32, 8), (32x64, 8); negative = not
+ * timed yet.
  * Returns the number of classes. */
 int tsc_autotune_table(tsc_ctx* ctx, int* cls, double* ms_per_gflop, int max_classes);
 /* Times every candidate schedule on the current superblock now (best of reps

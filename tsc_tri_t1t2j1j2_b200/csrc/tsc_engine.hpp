@@ -154,7 +154,7 @@ struct TaskList {
   GTerm* d_terms = nullptr;
   GReduce* d_reds = nullptr;
   int njobs = 0, nreds = 0;
-  int tile = 64;           // CTA tile edge used for this list (64 or 32)
+  int tile = 64;           // CTA tile code used for this list (TILE_* in tsc_kernels.cuh)
   bool split = false;      // jobs are 128 x 64 tiles for the split-precision kernel
   long long max_red_elems = 0;
   DevBufP part;            // partial tiles of split groups
@@ -244,7 +244,7 @@ class Engine {
   bool in_warmup_ = false;    // set while the warm-up (infinite-lattice) steps run
 
   // Autotuner of the FP64 H.psi schedule: for each size class (log2 of the
-  // H.psi GFLOP, superblocks of >= 8 GFLOP) the candidate (tile edge, waves)
+  // H.psi GFLOP, superblocks of >= 8 GFLOP) the candidate (CTA tile, waves)
   // schedules are timed, one per superblock on its first H.psi, in device
   // milliseconds per algorithmic GFLOP; once all are timed the class keeps the
   // fastest.  tsc_set_autotune switches it off (schedule fixed, results
@@ -253,7 +253,7 @@ class Engine {
     int tile, waves;
   };
   static constexpr int kTuneCands = 4;
-  const TuneCand tune_cands_[kTuneCands] = {{32, 4}, {32, 2}, {32, 8}, {64, 4}};
+  const TuneCand tune_cands_[kTuneCands] = {{TILE_32x32, 4}, {TILE_32x32, 8}, {TILE_64x32, 8}, {TILE_32x64, 8}};
   std::map<int, std::array<double, kTuneCands>> tune_ms_;   // class -> ms/GFLOP (<0: not timed)
   bool autotune_ = true;
   cudaEvent_t tune_ev_[2] = {nullptr, nullptr};   // bracket the candidate's H.psi

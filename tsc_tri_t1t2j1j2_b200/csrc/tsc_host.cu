@@ -504,15 +504,9 @@ int TaskList::add_group(double2* abs_c, uint8_t base, long long c_off, int ld, i
   return (int)groups.size() - 1;
 }
 
-// CTA tile edge of the grouped GEMM: 32x32 (6 CTAs/SM) by default; TSC_TILE=64
-// selects 64x64 tiles (2 CTAs/SM), kept for comparison.
-int default_tile() {
-  static int t = [] {
-    const char* e = std::getenv("TSC_TILE");
-    return (e && std::atoi(e) == 64) ? 64 : 32;
-  }();
-  return t;
-}
+// CTA tile of the grouped GEMM when no schedule is chosen: 32x32 (6 CTAs/SM);
+// the autotuner (Engine::tune_*) picks among 32x32, 64x32 and 32x64 per size class.
+int default_tile() { return TILE_32x32; }
 
 void TaskList::upload_split(cudaStream_t st) {
   split = true;
@@ -521,12 +515,13 @@ void TaskList::upload_split(cudaStream_t st) {
 
 void TaskList::upload(cudaStream_t st, int slots, int waves, int tile_override) {
   tile = tile_override ? tile_override : default_tile();
-  int TMt = tile, TNt = tile;
+  int TMt, TNt;
+  tile_dims(tile, TMt, TNt);
   if (split) {
     TMt = SPLIT_TILE_M;
     TNt = SPLIT_TILE_N;
-  } else if (tile == 32) {
-    slots *= 3;
+  } else {
+    slots = slots / 2 * (tile == TILE_32x32 ? 6 : tile == TILE_64x64 ? 2 : 4);   // resident CTAs per SM x SMs
   }
   std::vector<GTerm> terms;
   struct JC {

@@ -605,8 +605,12 @@ cudaError_t launch_tile(const GJob* jobs, int njobs, const GGroup* groups, const
 cudaError_t launch_grouped_zgemm(const GJob* jobs, int njobs, const GGroup* groups, const GTerm* terms,
                                  Bases bases, cudaStream_t st, int tile) {
   if (njobs <= 0) return cudaSuccess;
-  if (tile == 32) return launch_tile<32, 32, 6>(jobs, njobs, groups, terms, bases, st);
-  return launch_tile<64, 64, 2>(jobs, njobs, groups, terms, bases, st);
+  switch (tile) {
+    case TILE_32x32: return launch_tile<32, 32, 6>(jobs, njobs, groups, terms, bases, st);
+    case TILE_64x32: return launch_tile<64, 32, 4>(jobs, njobs, groups, terms, bases, st);
+    case TILE_32x64: return launch_tile<32, 64, 4>(jobs, njobs, groups, terms, bases, st);
+    default: return launch_tile<64, 64, 2>(jobs, njobs, groups, terms, bases, st);
+  }
 }
 
 cudaError_t launch_reduce_partials(const GReduce* reds, int nred, const GGroup* groups, Bases bases,

@@ -68,6 +68,12 @@ cudaError_t launch_grouped_zgemm_split(const GJob* jobs, int njobs, const GGroup
 // bounded mbarrier waits runs out.
 cudaError_t split_fault_flag(int* host_flag, int clear);
 constexpr int SPLIT_TILE_M = 128, SPLIT_TILE_N = 64;
+// CTA tile codes of launch_grouped_zgemm (rows x columns of the output tile)
+constexpr int TILE_32x32 = 32, TILE_64x64 = 64, TILE_64x32 = 6432, TILE_32x64 = 3264;
+inline void tile_dims(int code, int& tm, int& tn) {
+  tm = code == TILE_64x32 || code == TILE_64x64 ? 64 : 32;
+  tn = code == TILE_32x64 || code == TILE_64x64 ? 64 : 32;
+}
 
 // Sets a kernel's dynamic shared-memory limit once per device (the attribute
 // belongs to the current device's context; concurrent first calls set the same

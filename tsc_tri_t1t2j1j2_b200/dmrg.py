@@ -131,18 +131,18 @@ class Context:
         self._check(self.L.tsc_set_autotune(self.h, 1 if on else 0))
 
     def autotune_table(self):
-        """{size class (floor log2 GFLOP): ms per GFLOP of the candidates
-        (tile 32 / 4 waves, 32 / 2, 32 / 8, 64 / 4), None where not timed}."""
+        """{size class (floor log2 GFLOP): ms per GFLOP of TUNE_CANDIDATES,
+        None where not timed}."""
         cls = (ctypes.c_int * 64)()
         ms = (ctypes.c_double * 256)()
         n = self._check(self.L.tsc_autotune_table(self.h, cls, ms, 64))
         return {cls[i]: [ms[4 * i + c] if ms[4 * i + c] >= 0 else None for c in range(4)] for i in range(min(n, 64))}
 
-    TUNE_CANDIDATES = ((32, 4), (32, 2), (32, 8), (64, 4))   # (CTA tile edge, waves)
+    TUNE_CANDIDATES = (("32x32", 4), ("32x32", 8), ("64x32", 8), ("32x64", 8))   # (CTA tile, waves)
 
     def autotune_superblock(self, reps: int = 3):
         """Times every candidate H.psi schedule on the current superblock and keeps
-        the fastest; returns its (tile edge, waves)."""
+        the fastest; returns its (CTA tile, waves)."""
         return self.TUNE_CANDIDATES[self._check(self.L.tsc_autotune_superblock(self.h, int(reps)))]
 
     def hpsi_noalloc(self, d_in: int, d_out: int):
