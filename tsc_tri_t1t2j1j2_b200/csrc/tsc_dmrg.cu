@@ -129,43 +129,6 @@ constexpr int S_ALPHA = 0, S_BETA = 128, S_UV = 256, S_UU = 384, S_RES = 512, S_
 // Density-matrix eigenvalues below this are rounding noise (rho has unit trace).
 constexpr double kZeroWeight = 1e-13;
 
-// Kept states of zero weight: the reference keeps whatever null-space vectors
-// its LAPACK returns (den_mat.f90:395-396), which differ between eigensolvers.
-// Here they are a canonical orthonormal basis of the complement of the kept
-// significant eigenvectors Q (d x s): Gram-Schmidt of e_0, e_1, ... in order,
-// keeping candidates whose projected norm exceeds a threshold.  The result
-// depends on Q only through its projector.
-void null_completion(int d, int s, const cplx* Q, int m, cplx* N) {
-  int got = 0;
-  std::vector<cplx> v(d);
-  for (double thr : {0.5, 0.1, 1e-3}) {
-    for (int j = 0; j < d && got < m; ++j) {
-      std::fill(v.begin(), v.end(), cplx(0.0));
-      v[j] = 1.0;
-      for (int pass = 0; pass < 2; ++pass) {
-        for (int q = 0; q < s; ++q) {
-          cplx dot = 0.0;
-          for (int r = 0; r < d; ++r) dot += std::conj(Q[(size_t)q * d + r]) * v[r];
-          for (int r = 0; r < d; ++r) v[r] -= dot * Q[(size_t)q * d + r];
-        }
-        for (int q = 0; q < got; ++q) {
-          cplx dot = 0.0;
-          for (int r = 0; r < d; ++r) dot += std::conj(N[(size_t)q * d + r]) * v[r];
-          for (int r = 0; r < d; ++r) v[r] -= dot * N[(size_t)q * d + r];
-        }
-      }
-      double nrm = 0.0;
-      for (int r = 0; r < d; ++r) nrm += std::norm(v[r]);
-      nrm = std::sqrt(nrm);
-      if (nrm <= thr) continue;
-      for (int r = 0; r < d; ++r) N[(size_t)got * d + r] = v[r] / nrm;
-      got++;
-    }
-    if (got >= m) return;
-  }
-  throw Error(-1, "null_completion: complement too small");
-}
-
 // QuickSort_Double, block.f90:2398-2444 (descending with an index array)
 void quicksort_double(std::vector<double>& a, std::vector<int>& idx, int lo, int hi) {
   int i = lo, j = hi;
@@ -455,7 +418,7 @@ void Engine::truncate(int side, const double2* d_psi, const WLayout& wl, int kep
   cuda_check(cudaStreamSynchronize(st), "sync");
   for (int k = 0; k < wl.num; ++k)
     if (infoh[k] != 0) throw Error(-3, "zheevd did not converge");
-  // eigenvalues at rounding-noise level count as exact zeros (null_completion)
+  // eigenvalues at rounding-noise level count as exact zeros (see null_complete)
   for (int i = 1; i <= dim; ++i)
     if (evh[i] < kZeroWeight) evh[i] = 0.0;
   // den_mat.f90:249-333 on the host (scalars only)
@@ -523,6 +486,9 @@ void Engine::truncate(int side, const double2* d_psi, const WLayout& wl, int kep
   U.num = (int)U.sub.size();
   U.len = side == 0 ? wl.sys_len : wl.env_len;
   U.buf = std::make_shared<DevBuf>((size_t)std::max<long long>(uo, 1), st, false);
+  // kept columns of every sector; kept zero-weight columns are then replaced by
+  // the canonical complement basis on the GPU (null_complete)
+  std::vector<NullJob> nulls;
   int ui = 0;
   for (int k = 0; k < wl.num; ++k) {
     if (cnt[k] <= 0) continue;
@@ -531,26 +497,13 @@ void Engine::truncate(int side, const double2* d_psi, const WLayout& wl, int kep
     int sig = 0;
     for (int c = 0; c < col; ++c)
       if (evh[sidx0[k] + row - col + c] > 0.0) sig++;
-    if (sig == col) {
-      cuda_check(cudaMemcpyAsync(U.buf->p + s.off, den->p + doff[k] + (long long)(row - col) * row,
-                                 (size_t)row * col * sizeof(double2), cudaMemcpyDeviceToDevice, st),
-                 "U copy");
-    } else {
-      // kept zero-weight columns: canonical null-space basis (rare; host side)
-      std::vector<cplx> h((size_t)row * col);
-      cuda_check(cudaMemcpyAsync(h.data(), den->p + doff[k] + (long long)(row - col) * row,
-                                 (size_t)row * col * sizeof(double2), cudaMemcpyDeviceToHost, st),
-                 "U d2h");
-      cuda_check(cudaStreamSynchronize(st), "sync");
-      std::vector<cplx> nul((size_t)row * (col - sig));
-      null_completion(row, sig, h.data() + (size_t)(col - sig) * row, col - sig, nul.data());
-      std::copy(nul.begin(), nul.end(), h.begin());
-      cuda_check(cudaMemcpyAsync(U.buf->p + s.off, h.data(), h.size() * sizeof(double2), cudaMemcpyHostToDevice, st),
-                 "U h2d");
-      cuda_check(cudaStreamSynchronize(st), "sync");
-    }
+    cuda_check(cudaMemcpyAsync(U.buf->p + s.off, den->p + doff[k] + (long long)(row - col) * row,
+                               (size_t)row * col * sizeof(double2), cudaMemcpyDeviceToDevice, st),
+               "U copy");
+    if (sig < col) nulls.push_back(NullJob{U.buf->p + s.off, row, sig, col - sig});
     U.dim += col;
   }
+  null_complete(nulls);
   out.num_state = ns;
   out.err = err;
   out.ent = ent;

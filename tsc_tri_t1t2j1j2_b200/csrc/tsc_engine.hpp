@@ -278,6 +278,15 @@ class Engine {
   };
   void truncate(int side, const double2* d_psi, const WLayout& wl, int kept_min, int kept_max,
                 double trun_err, TruncResult& out);
+  // Kept zero-weight columns of one sector of U: W is the sector's d x (m + sig)
+  // block (ld d), m completion columns followed by the sig significant kept
+  // eigenvectors; the first m columns are overwritten by the canonical
+  // complement basis (tsc_nullspace.cu).
+  struct NullJob {
+    double2* W;
+    int d, sig, m;
+  };
+  void null_complete(const std::vector<NullJob>& jobs);
 
   // block growth + renormalisation (get_sys.f90:4-592)
   void grow(int side, DModel& pre, const Basis& basis, const DBlock& trun, int mshift);
