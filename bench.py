@@ -342,6 +342,9 @@ def sweep_leg(dev):
         t1 = time.perf_counter()
         dens = ctx.measure_density()
         meas_s = time.perf_counter() - t1
+        t1 = time.perf_counter()
+        cor = ctx.measure_density_cor(1)   # the wave ends at sys_len 2: site 1 with its leg partners
+        cor_s = time.perf_counter() - t1
         tuned = ctx.autotune_table()
         ctx.close()
         sw = [s for s in steps if s["phase"] != 0]
@@ -358,12 +361,21 @@ def sweep_leg(dev):
             "min_e0": min(s["e0"] for s in steps),
             "density_seconds": meas_s,
             "density": dens,
+            "density_cor_seconds": cor_s,
+            "density_cor": cor,
+            "trun_err": np.array([s["trun_err"] for s in steps]),
             "autotune_ms_per_gflop": {str(k): v for k, v in tuned.items()},
         }
     res["density_max_abs_diff_split_vs_fp64"] = float(np.max(np.abs(res["split"]["density"] - res["fp64"]["density"])))
     res["density_sum_fp64"] = float(res["fp64"]["density"].sum())
+    res["density_cor_site1_max_abs_diff_split_vs_fp64"] = float(
+        np.max(np.abs(res["split"]["density_cor"] - res["fp64"]["density_cor"])))
+    res["density_cor_site1_partners"] = int(np.count_nonzero(res["fp64"]["density_cor"]))
+    if len(res["split"]["trun_err"]) == len(res["fp64"]["trun_err"]):
+        res["trun_err_max_abs_diff_split_vs_fp64"] = float(
+            np.max(np.abs(res["split"]["trun_err"] - res["fp64"]["trun_err"])))
     for name in ("fp64", "split"):
-        del res[name]["density"]
+        del res[name]["density"], res[name]["density_cor"], res[name]["trun_err"]
     res["final_dE_over_E_split_vs_fp64"] = abs(res["split"]["final_e0"] - res["fp64"]["final_e0"]) / abs(
         res["fp64"]["final_e0"])
     res["sweep_speedup_split_over_fp64"] = res["fp64"]["sweep_seconds"] / res["split"]["sweep_seconds"]
@@ -380,7 +392,7 @@ def config1_leg(dev, with_cpu):
     with the CPU leg, the oracle (CPU restatement, OpenBLAS on all host cores)."""
     from tsc_tri_t1t2j1j2_b200 import Context
     res = {"workload": "YC4x6 t1=1 J1=0.4 t2=J2=0, warm-up m=100, 4 sweeps m=100,200,300,400, lanzero 1e-10"}
-    dens = {}
+    dens, cors = {}, {}
     for name, mode in (("fp64", Context.FP64), ("split", Context.SPLIT_BF16)):
         ctx = Context(device=dev.index, **CONFIG1)
         ctx.set_precision(mode, 1e-11)
@@ -388,6 +400,7 @@ def config1_leg(dev, with_cpu):
         steps = ctx.get_ground_state(**CONFIG1_RUN)
         res[name] = {"seconds": time.perf_counter() - t0, "steps": len(steps), "final_e0": steps[-1]["e0"]}
         dens[name] = ctx.measure_density()
+        cors[name] = ctx.measure_density_cor(1)
         ctx.close()
     if with_cpu:
         sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -399,11 +412,14 @@ def config1_leg(dev, with_cpu):
         ref = o.run()
         sec = time.perf_counter() - t0
         dref = o.measure_density()
+        cref = o.density_cor(1).real
         res["cpu_oracle"] = {"seconds": sec, "cores": os.cpu_count(), "steps": len(ref), "final_e0": ref[-1]["e0"]}
         res["fp64_final_dE_over_E_vs_oracle"] = abs(res["fp64"]["final_e0"] - ref[-1]["e0"]) / abs(ref[-1]["e0"])
         res["speedup_fp64_gpu_over_cpu"] = sec / res["fp64"]["seconds"]
         res["density_max_abs_diff_fp64_vs_oracle"] = float(np.max(np.abs(dens["fp64"] - dref)))
         res["density_max_abs_diff_split_vs_oracle"] = float(np.max(np.abs(dens["split"] - dref)))
+        res["density_cor_site1_max_abs_diff_fp64_vs_oracle"] = float(np.max(np.abs(cors["fp64"] - cref)))
+        res["density_cor_site1_max_abs_diff_split_vs_oracle"] = float(np.max(np.abs(cors["split"] - cref)))
         res["split_final_dE_over_E_vs_oracle"] = abs(res["split"]["final_e0"] - ref[-1]["e0"]) / abs(ref[-1]["e0"])
     return res
 

@@ -54,6 +54,8 @@ typedef struct tsc_sweep_config {
   double lanzero;          /* >0: Lanczos tolerance in every phase; <=0: reference schedule */
   unsigned long long seed; /* random initial states (block.f90:1154-1180 stand-in) */
   int warmup_only;         /* 1: stop after warm_up_point (dmrg_sub.f90:974-1147) */
+  int final_half_sweep;    /* 1: end with left_to_right up to 5*Num_site/6 (main.f90:205-206),
+                            * the position where the reference measures */
 } tsc_sweep_config;
 
 /* One record per Lanczos solve (eigen.f90:169-173, den_mat.f90:342-350). */
@@ -148,6 +150,17 @@ int tsc_dmrg_run(tsc_ctx* ctx, const tsc_sweep_config* sweep, tsc_step_log* log,
  * get_sys.f90:1147-1277) and measured on the last wavefunction.  Writes nsites
  * >= Nx*Ny values; returns the number written. */
 int tsc_measure_density(tsc_ctx* ctx, double* out, int nsites);
+
+/* Density-density correlations <n_site n_j> of the last ground state
+ * (Get_density_cor with oper1 = oper2 = num_elec, Flags 'B', xi = xj = site,
+ * measure.f90:2525-2681, main.f90:299).  `site` must lie in the system block of
+ * the last wavefunction (1 <= site <= sys_len - 1; the reference calls it with
+ * xi1 = (Nx/4)*Ny + 2 - Ny after the final half sweep that tsc_sweep_config's
+ * final_half_sweep runs).  The partners are the reference's: j = site + Ny,
+ * site + 2 Ny, ... up to min(Nx*Ny, Nx*Ny - Nx*Ny/6 + Ny).  Writes nsites >=
+ * Nx*Ny values, out[j-1] = Re <n_site n_j> for those j and 0 elsewhere (as the
+ * reference's zero-initialised correlation matrix row); returns Nx*Ny. */
+int tsc_measure_density_cor(tsc_ctx* ctx, int site, double* out, int nsites);
 
 /* Serialises the superblock of the most recent step of tsc_dmrg_run whose
  * global solve index equals capture_step (set before the run with

@@ -144,6 +144,16 @@ class Oracle {
   // (main.f90:89), Truns = .true.: site operator `st` of site old_idx carried
   // into the (truncated) block of length new_idx.
   Block oper_dia_in_block(const Block& st, int old_idx, int new_idx, bool sys);
+  // Get_density_cor (measure.f90:2525-2681) with oper1 = oper2 = num_elec, Flags
+  // 'B' and xi = xj = site (main.f90:299): <n_site n_j> of the last ground state
+  // for the partners j on the leg of `site` the reference visits (j = site + Ny,
+  // site + 2 Ny, ... up to Num_site - Num_site/6 + Ny), indexed 1..Num_site,
+  // zero where the reference computes nothing.
+  std::vector<cplx> density_cor(int site);
+  // Get_sys_oper_ndia / Get_env_oper_ndia (get_sys.f90:1536-1668), Types 'B'.
+  Block oper_ndia(const Block& st, int old_idx, int new_idx, bool sys, bool trunc);
+  // Change_sys/env_oper_ndia (get_sys.f90:1672-1778) or _dia (get_sys.f90:1281-1331), Truns.
+  Block change_oper(const Block& op, int old_idx, int new_idx, bool sys, bool ndia);
 
   // hot-path entry points restated (used directly by parity tests)
   void model_wave(Model& sys, Model& env, const Basis& sys_bs, const Basis& env_bs,

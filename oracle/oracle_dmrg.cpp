@@ -1143,3 +1143,332 @@ std::vector<double> Oracle::measure_density() {
 }
 
 }  // namespace orc
+
+// ---- density-density correlation (Get_density_cor, measure.f90:2525-2681) ---------
+
+namespace orc {
+namespace {
+
+// block_mul_block_ndia (block.f90:376-635) with Flag1 = Flag2 = 'N', coef = 1 and
+// new_oper%down_dif = 0, for two operators that conserve both quantum numbers
+// (up_dif = down_dif = 0): the 3j sums of block.f90:584-613 evaluated as written.
+Block block_mul_rank0(const Block& o1, const Block& o2, const Basis& basis) {
+  if (o1.up_dif || o2.up_dif || o1.down_dif || o2.down_dif)
+    throw std::runtime_error("block_mul_rank0: operators must conserve both quantum numbers");
+  Block nb;
+  nb.len = basis.len;
+  for (int i = 0; i < basis.num; ++i) {
+    const int num_up = basis.sub[i].new_num_up, num_down = basis.sub[i].new_num_down;
+    const int new_num_down = num_down;
+    const int bs_idx = find_bs(basis, num_up, new_num_down);
+    if (bs_idx < 0) continue;
+    SubBlock s;
+    s.num_up = num_up;
+    s.num_down = num_down;
+    s.down_dif = 0;
+    s.row_dim = basis.sub[bs_idx].dim;
+    s.sdim = basis.sub[i].dim;
+    s.mat.assign((size_t)s.row_dim * s.sdim, czero);
+    const int mid_num_down = num_down;
+    const int idx2 = find_blk3(o2, num_up, num_down, 0);
+    const int idx1 = find_blk3(o1, num_up, mid_num_down, 0);
+    if (idx1 >= 0 && idx2 >= 0) {
+      const int kq = -(-new_num_down) - num_down;   // j5 = -j4 - j6 of the normalising 3j
+      const double c11 = w3js(new_num_down, 0, num_down, -new_num_down, kq, num_down);
+      if (c11 == 0.0) throw std::runtime_error("block_mul_rank0: vanishing 3j normalisation");
+      double c1 = 0.0;
+      for (int m6 = -mid_num_down; m6 <= mid_num_down; m6 += 2) {
+        const int m5 = new_num_down - m6;
+        double c12 = w3js(new_num_down, 0, mid_num_down, -new_num_down, m5, m6);
+        const int m44 = -m6, m55 = -m44 - num_down;
+        c12 *= w3js(mid_num_down, 0, num_down, m44, m55, num_down) * pm1((mid_num_down + m44) / 2);
+        c12 *= w3js(0, 0, 0, m5, m55, -kq) * pm1(kq / 2) * std::sqrt(1.0);
+        c1 += c12;
+      }
+      if (c1 != 0.0) {
+        const SubBlock& a = o1.sub[idx1];
+        const SubBlock& b = o2.sub[idx2];
+        zgemm('N', 'N', s.row_dim, s.sdim, a.sdim, cplx(c1 / c11, 0.0), a.mat.data(), s.row_dim, b.mat.data(),
+              a.sdim, cone, s.mat.data(), s.row_dim);
+      }
+    }
+    nb.dim += s.sdim;
+    nb.sub.push_back(std::move(s));
+  }
+  nb.num = (int)nb.sub.size();
+  return nb;
+}
+
+const SubBasisMap* find_piece(const BasisMap& S, int bu, int bd, int su, int sd) {
+  for (const auto& p : S.sub)
+    if (p.bl_num_up == bu && p.bl_num_down == bd && p.st_num_up == su && p.st_num_down == sd) return &p;
+  return nullptr;
+}
+
+int find_wave(const Wave& w, int su, int sd, int eu, int ed) {
+  for (int m = 0; m < (int)w.sub.size(); ++m)
+    if (w.sub[m].sys_num_up == su && w.sub[m].sys_num_down == sd && w.sub[m].env_num_up == eu &&
+        w.sub[m].env_num_down == ed)
+      return m;
+  return -1;
+}
+
+// sys_block_site_cor_ndia (measure.f90:4064-4218), FlagSign 'B'
+cplx block_site_cor(const Block& bl, const Block& st, const Basis& bs, const Wave& w) {
+  const int K = bl.down_dif, up_dif = bl.up_dif;
+  cplx value = 0.0;
+  std::vector<cplx> mid;
+  for (const auto& ws : w.sub) {
+    const int j = find_bs(bs, ws.sys_num_up, ws.sys_num_down);
+    if (j < 0) continue;
+    for (const auto& p : bs.sub[j].sub)
+      for (int dd = -K; dd <= K; dd += 2)
+        for (int sdd = -K; sdd <= K; sdd += 2) {
+          const int nbu = p.bl_num_up + up_dif, nbd = p.bl_num_down + dd;
+          const int nsu = p.st_num_up - up_dif, nsd = p.st_num_down - sdd;
+          const int bid = find_blk3(bl, p.bl_num_up, p.bl_num_down, dd);
+          const int sid = find_blk3(st, nsu, nsd, sdd);
+          const SubBasisMap* q = find_piece(bs.sub[j], nbu, nbd, nsu, nsd);
+          if (bid < 0 || sid < 0 || !q) continue;
+          double c = 1.0 / std::sqrt(1.0 + K) * w6js(nbd, p.bl_num_down, K, p.st_num_down, nsd, ws.sys_num_down);
+          if (c == 0.0) continue;
+          c *= pm1((p.bl_num_down + nsd + K + ws.sys_num_down) / 2);
+          const cplx coef = st.sub[sid].mat[0] * c;
+          mid.assign((size_t)q->sdim * ws.env_dim, czero);
+          zgemm('N', 'N', q->sdim, ws.env_dim, p.sdim, coef, bl.sub[bid].mat.data(), q->sdim, ws.vec.data() + p.spos,
+                ws.sys_dim, czero, mid.data(), q->sdim);
+          for (int z = 0; z < ws.env_dim; ++z)
+            for (int r = 0; r < q->sdim; ++r)
+              value += std::conj(ws.vec[(size_t)z * ws.sys_dim + q->spos + r]) * mid[(size_t)z * q->sdim + r];
+        }
+  }
+  return value;
+}
+
+// sys_block_env_site_cor_ndia (measure.f90:4666-4903), FlagSign 'B'
+cplx block_env_site_cor(const Block& bl, const Block& est, const Basis& sbs, const Basis& ebs, const Wave& w) {
+  const int K = bl.down_dif, Ke = est.down_dif, up_dif = bl.up_dif;
+  cplx value = 0.0;
+  std::vector<cplx> mat;
+  for (const auto& ws : w.sub) {
+    const int j = find_bs(sbs, ws.sys_num_up, ws.sys_num_down), k = find_bs(ebs, ws.env_num_up, ws.env_num_down);
+    if (j < 0 || k < 0) continue;
+    for (const auto& x : sbs.sub[j].sub)
+      for (const auto& y : ebs.sub[k].sub)
+        for (int bdd = -K; bdd <= K; bdd += 2) {
+          const int nsbu = x.bl_num_up + up_dif, nsbd = x.bl_num_down + bdd;
+          const int sys_id = find_blk3(bl, x.bl_num_up, x.bl_num_down, bdd);
+          for (int sdd = -Ke; sdd <= Ke; sdd += 2) {
+            const int neu = y.st_num_up - up_dif, ned = y.st_num_down - sdd;
+            const int env_id = find_blk3(est, neu, ned, sdd);
+            if (sys_id < 0 || env_id < 0) continue;
+            for (int nsd = std::abs(ws.sys_num_down - K); nsd <= ws.sys_num_down + K; nsd += 2) {
+              const int nsu = ws.sys_num_up + up_dif, nenu = ws.env_num_up - up_dif, nend = nsd;
+              const int m1 = find_bs(sbs, nsu, nsd), m2 = find_bs(ebs, nenu, nend);
+              const SubBasisMap* qs = m1 < 0 ? nullptr : find_piece(sbs.sub[m1], nsbu, nsbd, x.st_num_up, x.st_num_down);
+              const SubBasisMap* qe = nullptr;
+              if (m2 >= 0)
+                for (const auto& p : ebs.sub[m2].sub)
+                  if (p.st_num_up == neu && p.st_num_down == ned && p.bl_num_down == y.bl_num_down) {
+                    qe = &p;
+                    break;
+                  }
+              const int wid = find_wave(w, nsu, nsd, nenu, nend);
+              if (!qs || !qe || wid < 0) continue;
+              double c = w6js(nsd, K, ws.sys_num_down, x.bl_num_down, x.st_num_down, nsbd);
+              if (c == 0.0) continue;
+              c *= w6js(nend, K, ws.env_num_down, y.st_num_down, y.bl_num_down, ned);
+              if (c == 0.0) continue;
+              c *= std::sqrt((1.0 + nend) * (1.0 + ws.env_num_down) / (1.0 + K));
+              if ((((nsbd + x.st_num_down + ws.sys_num_down + K) / 2 + (y.bl_num_down + y.st_num_down + nend + K) / 2) %
+                   2) != 0)
+                c = -c;
+              const cplx coef = est.sub[env_id].mat[0] * c;
+              mat.assign((size_t)qs->sdim * y.sdim, czero);
+              zgemm('N', 'N', qs->sdim, y.sdim, x.sdim, coef, bl.sub[sys_id].mat.data(), qs->sdim,
+                    ws.vec.data() + (size_t)y.spos * ws.sys_dim + x.spos, ws.sys_dim, czero, mat.data(), qs->sdim);
+              const SubWave& nw = w.sub[wid];
+              for (int m = 0; m < y.sdim; ++m)
+                for (int r = 0; r < qs->sdim; ++r)
+                  value += std::conj(nw.vec[(size_t)(qe->spos + m) * nw.sys_dim + qs->spos + r]) * mat[(size_t)m * qs->sdim + r];
+            }
+          }
+        }
+  }
+  return value;
+}
+
+// sys_block_env_block_cor_ndia (measure.f90:4398-4661), FlagSign 'B'
+cplx block_env_block_cor(const Block& bl, const Block& ebl, const Basis& sbs, const Basis& ebs, const Wave& w) {
+  const int K = bl.down_dif, up_dif = bl.up_dif;
+  cplx value = 0.0;
+  std::vector<cplx> mat1, mat2;
+  for (const auto& ws : w.sub) {
+    const int j = find_bs(sbs, ws.sys_num_up, ws.sys_num_down), k = find_bs(ebs, ws.env_num_up, ws.env_num_down);
+    if (j < 0 || k < 0) continue;
+    for (const auto& x : sbs.sub[j].sub)
+      for (const auto& y : ebs.sub[k].sub)
+        for (int dd = -K; dd <= K; dd += 2) {
+          const int nsbu = x.bl_num_up + up_dif, nsbd = x.bl_num_down + dd;
+          const int sys_id = find_blk3(bl, x.bl_num_up, x.bl_num_down, dd);
+          for (int edd = -K; edd <= K; edd += 2) {
+            const int nebu = y.bl_num_up - up_dif, nebd = y.bl_num_down - edd;
+            const int env_id = find_blk3(ebl, nebu, nebd, edd);
+            if (sys_id < 0 || env_id < 0) continue;
+            for (int nsd = std::abs(ws.sys_num_down - K); nsd <= ws.sys_num_down + K; nsd += 2) {
+              const int nsu = ws.sys_num_up + up_dif, nenu = ws.env_num_up - up_dif, nend = nsd;
+              const int m1 = find_bs(sbs, nsu, nsd), m2 = find_bs(ebs, nenu, nend);
+              const SubBasisMap* qs = m1 < 0 ? nullptr : find_piece(sbs.sub[m1], nsbu, nsbd, x.st_num_up, x.st_num_down);
+              const SubBasisMap* qe = m2 < 0 ? nullptr : find_piece(ebs.sub[m2], nebu, nebd, y.st_num_up, y.st_num_down);
+              const int wid = find_wave(w, nsu, nsd, nenu, nend);
+              if (!qs || !qe || wid < 0) continue;
+              double c = w6js(nsd, K, ws.sys_num_down, x.bl_num_down, x.st_num_down, nsbd);
+              if (c == 0.0) continue;
+              c *= w6js(nend, K, ws.env_num_down, y.bl_num_down, y.st_num_down, nebd);
+              if (c == 0.0) continue;
+              c *= std::sqrt((1.0 + nend) * (1.0 + ws.env_num_down) / (1.0 + K));
+              if ((((nsbd + x.st_num_down + ws.sys_num_down + K) / 2 + (nebd + y.st_num_down + ws.env_num_down + K) / 2) %
+                   2) == 1)
+                c = -c;
+              const SubWave& nw = w.sub[wid];
+              mat1.assign((size_t)qs->sdim * y.sdim, czero);
+              mat2.assign((size_t)qs->sdim * y.sdim, czero);
+              zgemm('N', 'N', qs->sdim, y.sdim, x.sdim, cone, bl.sub[sys_id].mat.data(), qs->sdim,
+                    ws.vec.data() + (size_t)y.spos * ws.sys_dim + x.spos, ws.sys_dim, czero, mat1.data(), qs->sdim);
+              zgemm('N', 'C', qs->sdim, y.sdim, qe->sdim, cplx(c, 0.0),
+                    nw.vec.data() + (size_t)qe->spos * nw.sys_dim + qs->spos, nw.sys_dim, ebl.sub[env_id].mat.data(),
+                    y.sdim, czero, mat2.data(), qs->sdim);
+              for (size_t e = 0; e < mat1.size(); ++e) value += std::conj(mat1[e]) * mat2[e];
+            }
+          }
+        }
+  }
+  return value;
+}
+
+}  // namespace
+
+// Get_sys_oper_ndia / Get_env_oper_ndia (get_sys.f90:1536-1668), trun_idx = 1,
+// Types 'B'; with trunc the result is truncated at the longer length (Truns).
+Block Oracle::oper_ndia(const Block& st, int old_idx, int new_idx, bool sys, bool trunc) {
+  const auto& bsm = sys ? sys_bsm : env_bsm;
+  const auto& truns = sys ? sys_truns : env_truns;
+  const int trun_idx = 1;
+  const int one = std::min(old_idx, new_idx), two = std::max(old_idx, new_idx);
+  Block cur, mid, out;
+  if (one <= two - 1) {
+    if (one <= 1) {
+      cur = st;
+    } else if (one <= trun_idx) {
+      update_site_ndia(st, bsm.at(one), cur, 'B', !sys);
+    } else {
+      update_site_ndia(st, bsm.at(one), mid, 'B', !sys);
+      update_trun_ndia(mid, cur, truns.at(one));
+    }
+    int idx = one;
+    while (idx + 1 <= two - 1) {
+      update_block_ndia(cur, bsm.at(idx + 1), mid, 'B', !sys);
+      idx++;
+      if (idx <= trun_idx) cur = mid;
+      else update_trun_ndia(mid, cur, truns.at(idx));
+    }
+    update_block_ndia(cur, bsm.at(idx + 1), out, 'B', !sys);
+  } else {
+    if (one <= 1) out = st;
+    else update_site_ndia(st, bsm.at(two), out, 'B', !sys);
+  }
+  auto it = truns.find(two);
+  if (!trunc || it == truns.end()) return out;
+  Block t;
+  update_trun_ndia(out, t, it->second);
+  return t;
+}
+
+// Change_sys_oper_ndia (get_sys.f90:1672-1723; ndia) or Change_sys_oper_dia
+// (get_sys.f90:1281-1331; dia), and their env twins, with Truns = .true.
+Block Oracle::change_oper(const Block& op, int old_idx, int new_idx, bool sys, bool ndia) {
+  const auto& bsm = sys ? sys_bsm : env_bsm;
+  const auto& truns = sys ? sys_truns : env_truns;
+  const int trun_idx = 1;
+  const int one = std::min(old_idx, new_idx), two = std::max(old_idx, new_idx);
+  if (one == two) return op;
+  auto grow = [&](const Block& b, const Basis& bs, Block& o) {
+    if (ndia) update_block_ndia(b, bs, o, 'B', !sys);
+    else update_block_dia(b, bs, o);
+  };
+  auto trun = [&](const Block& b, Block& o, const Block& t) {
+    if (ndia) update_trun_ndia(b, o, t);
+    else update_trun_dia(b, o, t);
+  };
+  Block cur = op, mid, out;
+  int idx = one;
+  while (idx + 1 <= two - 1) {
+    grow(cur, bsm.at(idx + 1), mid);
+    idx++;
+    if (idx <= trun_idx) cur = mid;
+    else trun(mid, cur, truns.at(idx));
+  }
+  grow(cur, bsm.at(idx + 1), out);
+  auto it = truns.find(two);
+  if (it == truns.end()) return out;
+  Block t;
+  trun(out, t, it->second);
+  return t;
+}
+
+std::vector<cplx> Oracle::density_cor(int xi) {
+  const Wave& w = disk_wave;
+  const int N = L.num_site, ny = L.Ny, sl = w.sys_len, el = w.env_len;
+  if (xi < 1 || xi > sl - 1) throw std::runtime_error("density_cor: the site must lie in the system block");
+  std::vector<cplx> out(N + 1, czero);
+  // partners inside the system block: Get_sys2b + measure_sys_block
+  for (int j = xi + ny; j <= sl - 1; j += ny) {
+    Block a = oper_ndia(num_elec, xi, j, true, false);
+    Block b = oper_ndia(num_elec, j, j, true, false);
+    Block p = block_mul_rank0(a, b, sys_bsm.at(j));
+    Block q;
+    auto it = sys_truns.find(j);
+    if (j <= 1 || it == sys_truns.end()) q = p;
+    else update_trun_dia(p, q, it->second);
+    Block s = change_oper(q, j, sl - 1, true, false);
+    out[j] = measure_block(s, sys_bsm.at(sl), w, true);
+  }
+  const int last = N - N / 6 + ny;
+  if (sl > last) return out;
+  Block s1 = oper_ndia(num_elec, xi, xi, true, false);
+  if (xi > 1) {
+    auto it = sys_truns.find(xi);
+    if (it != sys_truns.end()) {
+      Block t;
+      update_trun_ndia(s1, t, it->second);
+      s1 = t;
+    }
+  }
+  Block sys_oper = change_oper(s1, xi, sl - 1, true, true);
+  for (int j = sl; j <= std::min(last, N); ++j) {
+    if ((j - xi) % ny != 0) continue;
+    cplx v = 0.0;
+    if (j == sl) {
+      v = block_site_cor(sys_oper, num_elec, sys_bsm.at(sl), w);
+    } else if (j == sl + 1) {
+      v = block_env_site_cor(sys_oper, num_elec, sys_bsm.at(sl), env_bsm.at(el), w);
+    } else {
+      const int e = N - j + 1;
+      Block e1 = oper_ndia(num_elec, e, e, false, false);
+      if (e > 1) {
+        auto it = env_truns.find(e);
+        if (it != env_truns.end()) {
+          Block t;
+          update_trun_ndia(e1, t, it->second);
+          e1 = t;
+        }
+      }
+      Block env_oper = change_oper(e1, e, el - 1, false, true);
+      v = block_env_block_cor(sys_oper, env_oper, sys_bsm.at(sl), env_bsm.at(el), w);
+    }
+    out[j] = v;
+  }
+  return out;
+}
+
+}  // namespace orc

@@ -500,7 +500,7 @@ extern "C" {
 
 void* orc_new(int Nx, int Ny, double t1, double t2, double J1, double J2, int delta, int kept_min,
               int kept_warm, const int* sweep_kept, int nsweeps, double lanzero_override,
-              unsigned long long seed, int capture_step) {
+              unsigned long long seed, int capture_step, int final_half_sweep) {
   OrcHandle* h = new OrcHandle();
   Config& c = h->cfg;
   c.Nx = Nx; c.Ny = Ny; c.t1 = t1; c.t2 = t2; c.J1 = J1; c.J2 = J2; c.delta = delta;
@@ -508,6 +508,7 @@ void* orc_new(int Nx, int Ny, double t1, double t2, double J1, double J2, int de
   c.sweep_kept_max.assign(sweep_kept, sweep_kept + nsweeps);
   c.lanzero_override = lanzero_override;
   c.seed = seed;
+  c.final_half_sweep = final_half_sweep != 0;
   try {
     h->o = new Oracle(c);
     h->o->capture_step = capture_step;
@@ -547,6 +548,24 @@ int orc_measure_density(void* hp, double* out) {
     std::vector<double> d = h->o->measure_density();
     std::copy(d.begin(), d.end(), out);
     return (int)d.size();
+  } catch (std::exception& e) {
+    h->err = e.what();
+    return -1;
+  }
+}
+
+// <n_site n_j> of the last ground state (Get_density_cor): 2 * num_site doubles
+// (re, im) for j = 1..num_site, zero where the reference computes nothing
+int orc_density_cor(void* hp, int site, double* out) {
+  OrcHandle* h = (OrcHandle*)hp;
+  if (!h->o) return -1;
+  try {
+    std::vector<orc::cplx> d = h->o->density_cor(site);
+    for (size_t j = 1; j < d.size(); ++j) {
+      out[2 * (j - 1)] = d[j].real();
+      out[2 * (j - 1) + 1] = d[j].imag();
+    }
+    return (int)d.size() - 1;
   } catch (std::exception& e) {
     h->err = e.what();
     return -1;

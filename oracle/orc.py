@@ -34,7 +34,7 @@ def lib():
         L = ctypes.CDLL(LIB_PATH)
         vp, i, d = ctypes.c_void_p, ctypes.c_int, ctypes.c_double
         L.orc_new.restype = vp
-        L.orc_new.argtypes = [i, i, d, d, d, d, i, i, i, ctypes.POINTER(i), i, d, ctypes.c_ulonglong, i]
+        L.orc_new.argtypes = [i, i, d, d, d, d, i, i, i, ctypes.POINTER(i), i, d, ctypes.c_ulonglong, i, i]
         L.orc_free.argtypes = [vp]
         L.orc_error.restype = ctypes.c_char_p
         L.orc_error.argtypes = [vp]
@@ -53,6 +53,8 @@ def lib():
         L.orc_hpsi_flat.restype = i
         L.orc_measure_density.argtypes = [vp, ctypes.POINTER(d)]
         L.orc_measure_density.restype = i
+        L.orc_density_cor.argtypes = [vp, i, ctypes.POINTER(d)]
+        L.orc_density_cor.restype = i
         _lib = L
     return _lib
 
@@ -72,6 +74,7 @@ class RunConfig:
     sweeps: list = field(default_factory=lambda: [100])
     lanzero: float = -1.0      # >0 overrides the reference's Lanczos tolerance schedule
     seed: int = 1
+    final_half_sweep: bool = False   # main.f90:205-206: end at 5 Num_site / 6 (the measuring position)
 
 
 STEP_FIELDS = ["phase", "sys_len", "env_len", "e0", "iters", "num_state", "trun_err",
@@ -83,7 +86,8 @@ class Oracle:
         L = lib()
         sk = (ctypes.c_int * max(1, len(cfg.sweeps)))(*cfg.sweeps)
         self.h = L.orc_new(cfg.Nx, cfg.Ny, cfg.t1, cfg.t2, cfg.J1, cfg.J2, cfg.delta, cfg.kept_min,
-                           cfg.kept_warm, sk, len(cfg.sweeps), cfg.lanzero, cfg.seed, capture_step)
+                           cfg.kept_warm, sk, len(cfg.sweeps), cfg.lanzero, cfg.seed, capture_step,
+                           1 if cfg.final_half_sweep else 0)
         err = L.orc_error(self.h)
         if err:
             raise RuntimeError(err.decode())
@@ -111,6 +115,16 @@ class Oracle:
         if n < 0:
             raise RuntimeError(L.orc_error(self.h).decode())
         return out
+
+    def density_cor(self, site):
+        """<n_site n_j>, j = 1..Num_site, of the last ground state (Get_density_cor,
+        measure.f90:2525-2681); zero where the reference computes nothing."""
+        L = lib()
+        out = np.zeros(2 * self.cfg.Nx * self.cfg.Ny, dtype=np.float64)
+        n = L.orc_density_cor(self.h, int(site), out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+        if n < 0:
+            raise RuntimeError(L.orc_error(self.h).decode())
+        return out[0::2] + 1j * out[1::2]
 
     def capture(self):
         """Flat (ints, complex) serialisation of the captured superblock."""

@@ -138,9 +138,12 @@ def tj_ground_state(Nx, Ny, t1, t2, J1, J2, sign_t=-1.0, penalty=10.0):
     # site densities <n_q> of the ground state (site q+1 in the lattice numbering)
     p = np.abs(v[:, 0]) ** 2
     dens = [float(sum(p[k] for k, (um, dm) in enumerate(states) if ((um | dm) >> q) & 1)) for q in range(ns)]
+    # density-density correlations <n_a n_b> (row a, column b; sites a+1, b+1)
+    occ = np.array([[((um | dm) >> q) & 1 for q in range(ns)] for (um, dm) in states], dtype=np.float64)
+    ncor = (occ.T * p) @ occ
     return {"Nx": Nx, "Ny": Ny, "t1": t1, "t2": t2, "J1": J1, "J2": J2, "n_sites": ns,
             "n_electrons": ne, "dim": n, "e0_S0": e - penalty * s2, "S2": s2, "sign_t": sign_t,
-            "density": dens}
+            "density": dens, "density_cor": ncor.tolist()}
 
 
 def main():

@@ -34,3 +34,31 @@ def test_density_matches_oracle(mode, lanzero, tol):
         ctx.close()
     assert np.max(np.abs(dens - ref)) <= tol
     assert abs(dens.sum() - round(ref.sum())) <= 1e-10
+
+
+def oracle_density_cor(lanzero, sites):
+    cfg = orc.RunConfig(Nx=4, Ny=4, t1=1.0, t2=0.3, J1=0.4, J2=0.036, lanzero=lanzero, final_half_sweep=True, **RUN)
+    o = orc.Oracle(cfg)
+    o.run()
+    return {s: o.density_cor(s).real for s in sites}
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("mode,lanzero,tol", [(Context.FP64, 1e-10, 1e-11), (Context.SPLIT_BF16, 1e-13, 1e-7)])
+def test_density_cor_matches_oracle(mode, lanzero, tol):
+    """tsc_measure_density_cor after the final half sweep (YC4x4: the wave ends at
+    sys_len 13) for sites 1-4, whose partners cover the four kinds of
+    Get_density_cor, against the oracle's restatement; tolerances as for <n_i>."""
+    sites = (1, 2, 3, 4)
+    ref = oracle_density_cor(lanzero, sites)
+    ctx = Context(4, 4, 1.0, 0.3, 0.4, 0.036)
+    try:
+        ctx.set_precision(mode, 1e-11)
+        ctx.get_ground_state(lanzero=lanzero, final_half_sweep=True, **RUN)
+        got = {s: ctx.measure_density_cor(s) for s in sites}
+    finally:
+        ctx.close()
+    for s in sites:
+        assert np.count_nonzero(ref[s]) >= 3
+        assert np.max(np.abs(got[s] - ref[s])) <= tol, s
+        assert np.array_equal(got[s] == 0, ref[s] == 0)

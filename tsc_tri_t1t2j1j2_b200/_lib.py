@@ -20,7 +20,7 @@ EXPORTED = [
     "tsc_superblock_dim", "tsc_hpsi", "tsc_hpsi_device", "tsc_lanczos", "tsc_truncate",
     "tsc_renormalize", "tsc_wave_transform", "tsc_dmrg_run", "tsc_set_capture", "tsc_get_capture",
     "tsc_hpsi_stats", "tsc_stream", "tsc_hpsi_noalloc", "tsc_set_precision",
-    "tsc_blocksparse_set", "tsc_blocksparse_apply", "tsc_measure_density", "tsc_set_autotune",
+    "tsc_blocksparse_set", "tsc_blocksparse_apply", "tsc_measure_density", "tsc_measure_density_cor", "tsc_set_autotune",
     "tsc_autotune_table", "tsc_autotune_superblock",
 ]
 
@@ -33,7 +33,7 @@ class ModelConfig(ctypes.Structure):
 class SweepConfig(ctypes.Structure):
     _fields_ = [("kept_min", c_int), ("kept_max_warmup", c_int), ("nsweeps", c_int),
                 ("sweep_kept_max", P(c_int)), ("lanzero", c_double), ("seed", ctypes.c_ulonglong),
-                ("warmup_only", c_int)]
+                ("warmup_only", c_int), ("final_half_sweep", c_int)]
 
 
 class StepLog(ctypes.Structure):
@@ -91,6 +91,7 @@ def load():
                                       ctypes.POINTER(c_ll), ctypes.POINTER(c_double), ctypes.POINTER(c_double)]
     L.tsc_blocksparse_apply.argtypes = [c_void, c_void, c_void, c_int]
     L.tsc_measure_density.argtypes = [c_void, ctypes.POINTER(c_double), c_int]
+    L.tsc_measure_density_cor.argtypes = [c_void, c_int, ctypes.POINTER(c_double), c_int]
     L.tsc_set_autotune.argtypes = [c_void, c_int]
     L.tsc_autotune_table.argtypes = [c_void, ctypes.POINTER(c_int), ctypes.POINTER(c_double), c_int]
     L.tsc_autotune_superblock.argtypes = [c_void, c_int]

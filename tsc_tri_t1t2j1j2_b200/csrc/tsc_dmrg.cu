@@ -1448,7 +1448,7 @@ void Engine::right_to_left(int bg_id, int end_id, double trun_err, std::vector<S
 }
 
 void Engine::run(int kept_min, int kept_warm, const std::vector<int>& sweeps, double lanzero_override,
-                 unsigned long long seed, std::vector<StepRec>* log, bool warmup_only) {
+                 unsigned long long seed, std::vector<StepRec>* log, bool warmup_only, bool final_half) {
   const int N = L.num_site;
   rng = seed;
   nsolve_ = 0;
@@ -1478,6 +1478,8 @@ void Engine::run(int kept_min, int kept_warm, const std::vector<int>& sweeps, do
     left_to_right(1, N - 2, trun_err, log);
     right_to_left(N - 2, 1, trun_err, log);
   }
+  // main.f90:205-206: a last half sweep stops at 5 Num_site / 6, where Measurement reads the wave
+  if (final_half) left_to_right(1, 5 * N / 6 - 1, sweeps.empty() ? tmp_err : trun_err, log);
 }
 
 }  // namespace tsc

@@ -229,7 +229,13 @@ class Engine {
 
   // measurement of the last ground state (csrc/tsc_measure.cu, measure.f90)
   std::vector<double> measure_density();
-  DBlock oper_dia_in_block(const SiteOp& so, int old_idx, int new_idx, bool sys);
+  DBlock oper_dia_in_block(const SiteOp& so, int old_idx, int new_idx, bool sys, bool trunc = true);
+  // <n_site n_j> for the partners j of Get_density_cor (tsc_measure.cu)
+  std::vector<double> measure_density_cor(int site);
+  DBlock carry_dia(const DBlock& op, int from, int to, bool sys);
+  DBlock product_dia(const DBlock& a, const DBlock& b, const Basis& basis);
+  double corr_block_site(const DBlock& bl, const SiteOp& so, const Basis& bs);
+  double corr_block_env(const DBlock& bl, const DBlock* ebl, const SiteOp* eso, const Basis& sbs, const Basis& ebs);
   DBlock site_as_block(const SiteOp& so);
   DBlock site_dia(const SiteOp& so, const Basis& basis);
   DBlock block_dia(const DBlock& blk, const Basis& basis);
@@ -315,7 +321,7 @@ class Engine {
     double split_e0;
   };
   void run(int kept_min, int kept_warm, const std::vector<int>& sweeps, double lanzero_override,
-           unsigned long long seed, std::vector<StepRec>* log, bool warmup_only = false);
+           unsigned long long seed, std::vector<StepRec>* log, bool warmup_only = false, bool final_half = false);
   int capture_step = -1;
   struct Capture {
     bool valid = false;

@@ -217,10 +217,11 @@ class Context:
 
     # ------------------------------------------------------------------ full run
     def get_ground_state(self, kept_min, kept_warm, sweeps, lanzero=-1.0, seed=1, capture_step=-1, max_steps=100000,
-                         warmup_only=False):
+                         warmup_only=False, final_half_sweep=False):
         self._check(self.L.tsc_set_capture(self.h, capture_step))
         sk = (ctypes.c_int * max(1, len(sweeps)))(*sweeps)
-        cfg = _lib.SweepConfig(kept_min, kept_warm, len(sweeps), sk, lanzero, seed, 1 if warmup_only else 0)
+        cfg = _lib.SweepConfig(kept_min, kept_warm, len(sweeps), sk, lanzero, seed, 1 if warmup_only else 0,
+                               1 if final_half_sweep else 0)
         logs = (_lib.StepLog * max_steps)()
         n = self._check(self.L.tsc_dmrg_run(self.h, ctypes.byref(cfg), logs, max_steps))
         out = []
@@ -234,6 +235,18 @@ class Context:
         (measure_operator_dia, measure.f90:3-62)."""
         out = np.zeros(self.Nx * self.Ny, dtype=np.float64)
         self._check(self.L.tsc_measure_density(self.h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), len(out)))
+        return out
+
+    def measure_density_cor(self, site=None):
+        """<n_site n_j> (j = 1..Nx*Ny; zero where the reference computes nothing)
+        of the last ground state (Get_density_cor, measure.f90:2525-2681).  The
+        default site is the reference's xi1 = (Nx/4)*Ny + 2 - Ny (main.f90:255),
+        which needs the wave left by get_ground_state(..., final_half_sweep=True)."""
+        if site is None:
+            site = (self.Nx // 4) * self.Ny + 2 - self.Ny
+        out = np.zeros(self.Nx * self.Ny, dtype=np.float64)
+        self._check(self.L.tsc_measure_density_cor(self.h, int(site),
+                                                   out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), len(out)))
         return out
 
     def capture(self):
