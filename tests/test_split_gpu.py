@@ -92,3 +92,39 @@ def test_split_full_run_energies():
     e = np.array([s["e0"] for s in steps])[-tail:]
     er = np.array([s["e0"] for s in ref_steps])[-tail:]
     assert np.max(np.abs(e - er) / np.abs(er)) <= 1e-10
+
+
+@pytest.mark.gpu
+def test_split_error_against_inner_dimension():
+    """Error of one split product Y = X R^H (one sector, one term, the left
+    operator the identity) against the inner dimension K, entries N(0,1).
+    Measured on B200: normwise 3.9e-7 at K=16, 3.6e-6 at K=256, 5.5e-5 at
+    K=4096 -- growing like K, where the same product rounded to nearest in FP32
+    (numpy complex64) stays at ~3e-7.  The growth is the FP32 accumulator in
+    tensor memory losing a biased fraction of a unit in the last place on each
+    of the 12 MMAs a K=16 step adds into it.  Bounds: <= 1e-6 at K=16 and
+    <= 2e-4 at K=4096, and at least 8x growth between the two."""
+    import torch
+    from tsc_tri_t1t2j1j2_b200.blocksparse import Problem
+    rng = np.random.default_rng(5)
+    errs = {}
+    for K in (16, 4096):
+        d = 32
+        X = rng.normal(size=(d, K)) + 1j * rng.normal(size=(d, K))
+        R = rng.normal(size=(K, K)) + 1j * rng.normal(size=(K, K))
+        P = Problem(d=[d], e=[K], left=[(0, [np.eye(d, dtype=complex)])], right=[(0, [R])], terms=[(1.0 + 0j, 0, 0)])
+        ref = X @ R.conj().T
+        ctx = Context(3, 4)
+        try:
+            ctx.blocksparse_set([P])
+            xd = torch.from_numpy(X.ravel(order="F").copy()).cuda()
+            yd = torch.zeros_like(xd)
+            ctx.blocksparse_apply(xd.data_ptr(), yd.data_ptr(), SPLIT)
+            torch.cuda.synchronize()
+            y = yd.cpu().numpy().reshape((d, K), order="F")
+        finally:
+            ctx.close()
+        errs[K] = float(np.linalg.norm(y - ref) / np.linalg.norm(ref))
+    assert errs[16] <= 1e-6
+    assert errs[4096] <= 2e-4
+    assert errs[4096] >= 8 * errs[16]
