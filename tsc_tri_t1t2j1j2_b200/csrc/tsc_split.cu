@@ -8,9 +8,13 @@
 // (0,0) (0,1) (1,0) (1,1) (0,2) (2,0) -- run as tcgen05.mma kind::f16 with FP32
 // accumulators in tensor memory, and the complex product is assembled from four
 // real accumulations (Cr += Ar Br - Ai Bi, Ci += Ar Bi + Ai Br).  Each slice
-// product is exact in FP32; the accumulation rounds at 2^-24 of the running sum,
-// so the result carries about 1e-6 relative error against the FP64 product.
-// Element terms and the write-back (beta, partial tiles) are done in FP64.
+// product is exact in FP32, but every MMA that adds into an FP32 accumulator
+// loses a biased part of its last place, so one long chain gathers an error that
+// grows like K (5.5e-5 at K=4096 in one accumulator).  Hence two accumulators
+// per output -- the (0,0) pair alone ("hi") and the five pairs 2^-8 smaller
+// ("lo") -- restarted every SP_SEG K steps; the epilogue adds each segment into
+// the output in FP64.  Element terms and the write-back (beta, partial tiles)
+// are done in FP64.
 //
 // Persistent and warp-specialised: one CTA per SM walks the jobs blockIdx.x,
 // +gridDim.x, ... (128 x 64 output tiles of a group over a term range, in
@@ -20,9 +24,10 @@
 // for A and B) of a shared-memory stage in the canonical K-major, no-swizzle
 // UMMA layout, and arrive on the stage's full barrier; one lane of the MMA warp
 // issues the step's 24 MMAs into one of two TMEM accumulators and commits them
-// to the stage's empty barrier (and, after a job's last step, to the
-// accumulator's full barrier); 4 epilogue warps drain the other accumulator,
-// add the FP64 element terms and write the tile while the next job runs.
+// to the stage's empty barrier (and, after a segment's last step, to the
+// accumulator's full barrier); 4 epilogue warps drain the other accumulator
+// into the tile in FP64 (the first segment with beta and the element terms,
+// later ones adding to it) while the next segment runs.
 // Every mbarrier wait is bounded: on timeout the kernel raises a CTA abort flag
 // and a device fault flag, waits (bounded) for its own MMAs, frees its tensor
 // memory and returns.
@@ -44,7 +49,12 @@ constexpr int A_PLANE = SP_TM * SP_TK * 2;                     // bytes of one B
 constexpr int B_PLANE = SP_TN * SP_TK * 2;                     // ... of B
 constexpr int STAGE_BYTES = 6 * A_PLANE + 6 * B_PLANE;         // 36,864
 constexpr int SMEM_BYTES = SP_STAGES * STAGE_BYTES + 256;      // + mbarriers, TMEM slot, abort flag
-constexpr uint32_t TMEM_COLS = 4 * SP_TN;                      // two accumulators (Cr | Ci), FP32
+// Two accumulators (double buffer), each [Cr hi | Ci hi | Cr lo | Ci lo]: the
+// (0,0) slice pair alone in "hi", the five smaller pairs in "lo".  Both restart
+// every SP_SEG K steps; the epilogue adds each segment into the output in FP64,
+// so no FP32 chain in tensor memory is longer than 2 * SP_SEG MMAs (hi).
+constexpr int SP_SEG = 4;
+constexpr uint32_t TMEM_COLS = 8 * SP_TN;                      // 512: the whole of an SM's tensor memory
 constexpr long long WAIT_LIMIT = 1ll << 20;
 
 // instruction descriptor, kind::f16: D f32, A/B bf16, both K-major, N>>3, M>>4
@@ -106,6 +116,16 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatil
 
 __device__ __forceinline__ void fence_before_sync() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void fence_after_sync() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+__device__ __forceinline__ void tmem_ld8(uint32_t taddr, float* v) {
+  uint32_t r[8];
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+               : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 8; ++i) v[i] = __uint_as_float(r[i]);
+}
 
 __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
   uint32_t r[16];
@@ -364,19 +384,21 @@ grouped_zgemm_split_kernel(const GJob* __restrict__ jobs, int njobs, const GGrou
   } else if (warp == SP_MMA_WARP) {
     // ---------------------------------------------------------------- MMA issuer
     if (lane == 0) {
-      int q = 0, jl = 0;
+      int q = 0, sg = 0;   // stage use, accumulator segment (over the CTA's jobs)
       bool ok = true;
       for (int jb = blockIdx.x; jb < njobs && ok; jb += gridDim.x) {
         const int nst = job_steps(jobs[jb], terms);
-        if (nst == 0) continue;
-        const int a = jl & 1, ua = jl >> 1;
-        if (ua >= 1 && !mbar_wait(smem_u32(&acce[a]), (uint32_t)((ua - 1) & 1), abort_flag)) {
-          ok = false;
-          break;
-        }
-        fence_after_sync();
-        const uint32_t dcr = tmem + a * (2 * SP_TN), dci = dcr + SP_TN;
         for (int i = 0; i < nst; ++i, ++q) {
+          const int si = i % SP_SEG;
+          const int a = sg & 1, ua = sg >> 1;
+          if (si == 0) {   // a segment starts: wait until the epilogue has drained this accumulator
+            if (ua >= 1 && !mbar_wait(smem_u32(&acce[a]), (uint32_t)((ua - 1) & 1), abort_flag)) {
+              ok = false;
+              break;
+            }
+            fence_after_sync();
+          }
+          const uint32_t dhr = tmem + a * (4 * SP_TN), dhi = dhr + SP_TN, dlr = dhr + 2 * SP_TN, dli = dhr + 3 * SP_TN;
           const int s = q % SP_STAGES;
           if (!mbar_wait(smem_u32(&full[s]), (uint32_t)((q / SP_STAGES) & 1), abort_flag)) {
             ok = false;
@@ -389,17 +411,19 @@ grouped_zgemm_split_kernel(const GJob* __restrict__ jobs, int njobs, const GGrou
             const int sa = c_pairs[pi][0], sb = c_pairs[pi][1];
             const uint64_t ar = smem_desc(a0 + (2 * sa) * A_PLANE), ai = smem_desc(a0 + (2 * sa + 1) * A_PLANE);
             const uint64_t br = smem_desc(b0 + (2 * sb) * B_PLANE), bi = smem_desc(b0 + (2 * sb + 1) * B_PLANE);
-            const uint32_t first = (i == 0 && pi == 0) ? 0u : 1u;
+            const uint32_t dcr = pi == 0 ? dhr : dlr, dci = pi == 0 ? dhi : dli;
+            const uint32_t first = (si == 0 && pi <= 1) ? 0u : 1u;   // first write of hi (pi 0) and lo (pi 1)
             umma_bf16(dcr, ar, br, IDESC, first);          // Cr  = Ar Br
             umma_bf16(dcr, ai, bi, IDESC_NEG_A, 1u);       // Cr -= Ai Bi
             umma_bf16(dci, ar, bi, IDESC, first);          // Ci  = Ar Bi
             umma_bf16(dci, ai, br, IDESC, 1u);             // Ci += Ai Br
           }
           umma_commit(smem_u32(&empty[s]));
+          if (si == SP_SEG - 1 || i == nst - 1) {   // segment complete: hand it to the epilogue
+            umma_commit(smem_u32(&accf[a]));
+            sg++;
+          }
         }
-        if (!ok) break;
-        umma_commit(smem_u32(&accf[a]));
-        jl++;
       }
       if (!ok) fail();
       // every MMA issued here has completed before the accumulators are freed
@@ -409,95 +433,105 @@ grouped_zgemm_split_kernel(const GJob* __restrict__ jobs, int njobs, const GGrou
     __syncwarp();
   } else {
     // ---------------------------------------------------------------- epilogue
-    const int ew = warp - SP_EPI_WARP0;      // 0..3
     const int quad = warp & 3;               // TMEM lane quadrant this warp may read
-    int jl = 0;
-    for (int jb = blockIdx.x; jb < njobs; jb += gridDim.x) {
+    int sg = 0;
+    bool ok = true;
+    for (int jb = blockIdx.x; jb < njobs && ok; jb += gridDim.x) {
       const GJob job = jobs[jb];
       const GGroup g = groups[job.group];
       const int nst = job_steps(job, terms);
-      const int a = jl & 1, ua = jl >> 1;
-      if (nst > 0) {
-        if (!mbar_wait(smem_u32(&accf[a]), (uint32_t)(ua & 1), abort_flag)) {
-          fail();
-          break;
-        }
-        fence_after_sync();
-      }
+      const int nseg = (nst + SP_SEG - 1) / SP_SEG;
       const int m0 = job.tm * SP_TM, n0 = job.tn * SP_TN;
       const int row = m0 + quad * 32 + lane;
-      const uint32_t lane_base = tmem + a * (2 * SP_TN) + ((uint32_t)(quad * 32) << 16);
       const bool partial = job.part >= 0;
       double2* C = partial ? bases.part + job.part_off : bases.p[g.c_base] + g.c_off;
       const long long ldc = partial ? g.M : g.c_ld;
       const bool acc_old = !partial && g.beta;
+      // one pass per accumulator segment (one pass of zeros for a job of element terms only);
+      // the first writes beta * C_old + element terms + segment, later ones add to what it wrote
+      for (int sgi = 0; sgi < (nseg > 0 ? nseg : 1); ++sgi) {
+        const int a = sg & 1, ua = sg >> 1;
+        if (nseg > 0) {
+          if (!mbar_wait(smem_u32(&accf[a]), (uint32_t)(ua & 1), abort_flag)) {
+            fail();
+            ok = false;
+            break;
+          }
+          fence_after_sync();
+        }
+        const uint32_t lane_base = tmem + a * (4 * SP_TN) + ((uint32_t)(quad * 32) << 16);
 #pragma unroll 1
-      for (int cb = 0; cb < SP_TN / 16; ++cb) {
-        const int c0 = cb * 16;
-        float vr[16], vi[16];
-        __syncwarp();
-        if (nst > 0) {
-          tmem_ld16(lane_base + c0, vr);
-          tmem_ld16(lane_base + SP_TN + c0, vi);
-        } else {
-#pragma unroll
-          for (int j = 0; j < 16; ++j) vr[j] = vi[j] = 0.f;
-        }
-        if (nst > 0 && cb == SP_TN / 16 - 1) {   // accumulator read out: hand it back
-          fence_before_sync();
+        for (int cb = 0; cb < SP_TN / 8; ++cb) {
+          const int c0 = cb * 8;
+          double cr[8], ci[8];
           __syncwarp();
-          if (lane == 0) mbar_arrive(smem_u32(&acce[a]));
-        }
-        double cr[16], ci[16];
+          if (nseg > 0) {
+            float hr[8], hi[8], lr[8], li[8];
+            tmem_ld8(lane_base + c0, hr);
+            tmem_ld8(lane_base + SP_TN + c0, hi);
+            tmem_ld8(lane_base + 2 * SP_TN + c0, lr);
+            tmem_ld8(lane_base + 3 * SP_TN + c0, li);
 #pragma unroll
-        for (int j = 0; j < 16; ++j) {
-          cr[j] = vr[j];
-          ci[j] = vi[j];
-        }
-        // element terms (AXPY / DIAG) in FP64, as grouped_zgemm applies them
-        for (int ti = job.t0; ti < job.t1; ++ti) {
-          const GTerm t = terms[ti];
-          if (t.kind == TK_GEMM) continue;
-          const double2* R = bases.p[t.r_base] + t.r_off;
-          const int rr = row - t.r0;
-          if (row >= g.M || rr < 0 || rr >= t.rm) continue;
-#pragma unroll
-          for (int j = 0; j < 16; ++j) {
-            const int col = n0 + c0 + j, cc = col - t.c0;
-            if (col >= g.N || cc < 0 || cc >= t.rn) continue;
-            double xr, xi;
-            if (t.kind == TK_AXPY) {
-              const double2 x = (t.r_op == OP_N) ? R[(long long)rr + (long long)cc * t.r_ld]
-                                                 : R[(long long)cc + (long long)rr * t.r_ld];
-              xr = x.x;
-              xi = (t.r_op == OP_C) ? -x.y : x.y;
-            } else {
-              if (rr != cc) continue;
-              xr = 1.0;
-              xi = 0.0;
+            for (int j = 0; j < 8; ++j) {
+              cr[j] = (double)hr[j] + (double)lr[j];
+              ci[j] = (double)hi[j] + (double)li[j];
             }
-            cr[j] += t.ar * xr - t.ai * xi;
-            ci[j] += t.ar * xi + t.ai * xr;
+          } else {
+#pragma unroll
+            for (int j = 0; j < 8; ++j) cr[j] = ci[j] = 0.0;
+          }
+          if (nseg > 0 && cb == SP_TN / 8 - 1) {   // accumulator read out: hand it back
+            fence_before_sync();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(smem_u32(&acce[a]));
+          }
+          if (sgi == 0) {
+            // element terms (AXPY / DIAG) in FP64, as grouped_zgemm applies them
+            for (int ti = job.t0; ti < job.t1; ++ti) {
+              const GTerm t = terms[ti];
+              if (t.kind == TK_GEMM) continue;
+              const double2* R = bases.p[t.r_base] + t.r_off;
+              const int rr = row - t.r0;
+              if (row >= g.M || rr < 0 || rr >= t.rm) continue;
+#pragma unroll
+              for (int j = 0; j < 8; ++j) {
+                const int col = n0 + c0 + j, cc = col - t.c0;
+                if (col >= g.N || cc < 0 || cc >= t.rn) continue;
+                double xr, xi;
+                if (t.kind == TK_AXPY) {
+                  const double2 x = (t.r_op == OP_N) ? R[(long long)rr + (long long)cc * t.r_ld]
+                                                     : R[(long long)cc + (long long)rr * t.r_ld];
+                  xr = x.x;
+                  xi = (t.r_op == OP_C) ? -x.y : x.y;
+                } else {
+                  if (rr != cc) continue;
+                  xr = 1.0;
+                  xi = 0.0;
+                }
+                cr[j] += t.ar * xr - t.ai * xi;
+                ci[j] += t.ar * xi + t.ai * xr;
+              }
+            }
+          }
+          if (row < g.M) {
+            const bool add = sgi > 0 || acc_old;
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+              const int col = n0 + c0 + j;
+              if (col >= g.N) continue;
+              double2* p = C + (long long)row + (long long)col * ldc;
+              double2 v = make_double2(cr[j], ci[j]);
+              if (add) {
+                const double2 o = *p;
+                v.x += o.x;
+                v.y += o.y;
+              }
+              *p = v;
+            }
           }
         }
-        if (row < g.M) {
-#pragma unroll
-          for (int j = 0; j < 16; ++j) {
-            const int col = n0 + c0 + j;
-            if (col >= g.N) continue;
-            double2* p = C + (long long)row + (long long)col * ldc;
-            double2 v = make_double2(cr[j], ci[j]);
-            if (acc_old) {
-              const double2 o = *p;
-              v.x += o.x;
-              v.y += o.y;
-            }
-            *p = v;
-          }
-        }
+        if (nseg > 0) sg++;
       }
-      if (nst > 0) jl++;
-      (void)ew;
     }
   }
   fence_before_sync();
