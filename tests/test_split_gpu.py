@@ -102,9 +102,10 @@ def test_split_error_against_inner_dimension():
     place on each MMA, so one long chain grows like K (5.5e-5 at K=4096 when
     all slice pairs shared one accumulator for the whole K).  With the (0,0)
     pair in its own accumulator and both restarted every few K steps, drained
-    into FP64, the error stays flat: measured 5e-8 at K=16 and 1.2e-7 from
-    K=64 to K=4096, below the same product rounded to nearest in FP32 (numpy
-    complex64, 2.7e-7).  Bounds: <= 5e-7 at K=16 and <= 1e-6 at K=4096."""
+    into FP64, the error stays flat: measured 5e-8 at K=16, 1.2e-7 at K=64 and
+    2.3e-7 from K=256 to K=4096, as the same product rounded to nearest in
+    FP32 (numpy complex64, 2.1e-7 to 2.7e-7).  Bounds: <= 5e-7 at K=16 and
+    <= 1e-6 at K=4096."""
     import torch
     from tsc_tri_t1t2j1j2_b200.blocksparse import Problem
     rng = np.random.default_rng(5)

@@ -53,7 +53,7 @@ constexpr int SMEM_BYTES = SP_STAGES * STAGE_BYTES + 256;      // + mbarriers, T
 // (0,0) slice pair alone in "hi", the five smaller pairs in "lo".  Both restart
 // every SP_SEG K steps; the epilogue adds each segment into the output in FP64,
 // so no FP32 chain in tensor memory is longer than 2 * SP_SEG MMAs (hi).
-constexpr int SP_SEG = 4;
+constexpr int SP_SEG = 8;
 constexpr uint32_t TMEM_COLS = 8 * SP_TN;                      // 512: the whole of an SM's tensor memory
 constexpr long long WAIT_LIMIT = 1ll << 20;
 
@@ -514,19 +514,24 @@ grouped_zgemm_split_kernel(const GJob* __restrict__ jobs, int njobs, const GGrou
             }
           }
           if (row < g.M) {
-            const bool add = sgi > 0 || acc_old;
+            // all eight old values in flight before any store (the stores could alias them)
+            if (sgi > 0 || acc_old) {
+              double2 o[8];
+#pragma unroll
+              for (int j = 0; j < 8; ++j) {
+                const int col = n0 + c0 + j;
+                o[j] = col < g.N ? C[(long long)row + (long long)col * ldc] : make_double2(0.0, 0.0);
+              }
+#pragma unroll
+              for (int j = 0; j < 8; ++j) {
+                cr[j] += o[j].x;
+                ci[j] += o[j].y;
+              }
+            }
 #pragma unroll
             for (int j = 0; j < 8; ++j) {
               const int col = n0 + c0 + j;
-              if (col >= g.N) continue;
-              double2* p = C + (long long)row + (long long)col * ldc;
-              double2 v = make_double2(cr[j], ci[j]);
-              if (add) {
-                const double2 o = *p;
-                v.x += o.x;
-                v.y += o.y;
-              }
-              *p = v;
+              if (col < g.N) C[(long long)row + (long long)col * ldc] = make_double2(cr[j], ci[j]);
             }
           }
         }
