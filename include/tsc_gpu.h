@@ -182,8 +182,8 @@ void* tsc_stream(tsc_ctx* ctx);
 /* Arithmetic of the H.psi sector GEMMs (the reference computes everything in
  * complex FP64 and has no such switch).  TSC_FP64: complex FP64 throughout.
  * TSC_SPLIT_BF16: every FP64 operand split into three BF16 slices multiplied
- * on the tensor cores with FP32 accumulation (about 1e-6 relative error per
- * H.psi); Lanczos iterates on that H.psi until successive Ritz values agree to
+ * on the tensor cores with FP32 accumulators restarted every 128 of the inner
+ * dimension and summed in FP64 (a few 1e-7 relative error per H.psi); Lanczos iterates on that H.psi until successive Ritz values agree to
  * split_tol relative (<= 0 keeps the current value, 1e-9 at creation), then
  * runs the reference's FP64 iterations from that vector until the FP64
  * residual ||H psi - E psi|| is below 0.1 sqrt(lanzero), so the energy and

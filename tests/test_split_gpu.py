@@ -2,8 +2,8 @@
 finished in FP64) against the FP64 engine and the oracle, through the C-ABI.
 
 Tolerances: split H.psi max|dx|/max|x| <= 2e-5 against the FP64 H.psi (three
-BF16 slices with FP32 accumulation: ~1e-6 on physical superblocks, ~1.6e-5 on
-the random-valued YC4x12 m=1000 superblock); ground-state energy after the FP64
+BF16 slices, FP32 accumulators restarted every 128 of K and summed in FP64:
+3.8e-7 on the random-valued YC4x12 m=1000 superblock); ground-state energy after the FP64
 refinement |dE/E| <= 1e-10 against the oracle, for single solves and for the
 last quarter of the steps of a full small run at lanzero = 1e-13.
 """
