@@ -150,6 +150,11 @@ class Oracle {
   // site + 2 Ny, ... up to Num_site - Num_site/6 + Ny), indexed 1..Num_site,
   // zero where the reference computes nothing.
   std::vector<cplx> density_cor(int site);
+  // The same with oper1 = oper2 = st_sd (main.f90:275): <S_site . S_j>.
+  std::vector<cplx> spin_cor(int site);
+  // Get_density_cor for any 'B' operator (scaled by sqrt(1 + rank), negated for rank 1,
+  // measure.f90:2586-2587, 2662-2663).
+  std::vector<cplx> oper_cor(const Block& op, int site);
   // Get_sys_oper_ndia / Get_env_oper_ndia (get_sys.f90:1536-1668), Types 'B'.
   Block oper_ndia(const Block& st, int old_idx, int new_idx, bool sys, bool trunc);
   // Change_sys/env_oper_ndia (get_sys.f90:1672-1778) or _dia (get_sys.f90:1281-1331), Truns.

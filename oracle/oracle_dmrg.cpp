@@ -1149,54 +1149,81 @@ std::vector<double> Oracle::measure_density() {
 namespace orc {
 namespace {
 
-// block_mul_block_ndia (block.f90:376-635) with Flag1 = Flag2 = 'N', coef = 1 and
-// new_oper%down_dif = 0, for two operators that conserve both quantum numbers
-// (up_dif = down_dif = 0): the 3j sums of block.f90:584-613 evaluated as written.
-Block block_mul_rank0(const Block& o1, const Block& o2, const Basis& basis) {
-  if (o1.up_dif || o2.up_dif || o1.down_dif || o2.down_dif)
-    throw std::runtime_error("block_mul_rank0: operators must conserve both quantum numbers");
+// block_mul_block_ndia (block.f90:376-635) with Flag1 = Flag2 = 'N', coef = 1:
+// (o1 o2) coupled to rank new_down_dif on the sectors of `basis`, the 3j sums
+// of block.f90:584-613 evaluated as written.
+Block block_mul_ndia_nn(const Block& o1, const Block& o2, int new_down_dif, const Basis& basis) {
+  const int up_dif2 = o2.up_dif, K1 = o1.down_dif, K2 = o2.down_dif;
   Block nb;
   nb.len = basis.len;
+  nb.up_dif = o1.up_dif + o2.up_dif;
+  nb.down_dif = new_down_dif;
+  const int up_dif = nb.up_dif, down_dif = new_down_dif;
   for (int i = 0; i < basis.num; ++i) {
     const int num_up = basis.sub[i].new_num_up, num_down = basis.sub[i].new_num_down;
-    const int new_num_down = num_down;
-    const int bs_idx = find_bs(basis, num_up, new_num_down);
-    if (bs_idx < 0) continue;
-    SubBlock s;
-    s.num_up = num_up;
-    s.num_down = num_down;
-    s.down_dif = 0;
-    s.row_dim = basis.sub[bs_idx].dim;
-    s.sdim = basis.sub[i].dim;
-    s.mat.assign((size_t)s.row_dim * s.sdim, czero);
-    const int mid_num_down = num_down;
-    const int idx2 = find_blk3(o2, num_up, num_down, 0);
-    const int idx1 = find_blk3(o1, num_up, mid_num_down, 0);
-    if (idx1 >= 0 && idx2 >= 0) {
-      const int kq = -(-new_num_down) - num_down;   // j5 = -j4 - j6 of the normalising 3j
-      const double c11 = w3js(new_num_down, 0, num_down, -new_num_down, kq, num_down);
-      if (c11 == 0.0) throw std::runtime_error("block_mul_rank0: vanishing 3j normalisation");
-      double c1 = 0.0;
-      for (int m6 = -mid_num_down; m6 <= mid_num_down; m6 += 2) {
-        const int m5 = new_num_down - m6;
-        double c12 = w3js(new_num_down, 0, mid_num_down, -new_num_down, m5, m6);
-        const int m44 = -m6, m55 = -m44 - num_down;
-        c12 *= w3js(mid_num_down, 0, num_down, m44, m55, num_down) * pm1((mid_num_down + m44) / 2);
-        c12 *= w3js(0, 0, 0, m5, m55, -kq) * pm1(kq / 2) * std::sqrt(1.0);
-        c1 += c12;
-      }
-      if (c1 != 0.0) {
+    const int new_num_up = num_up + up_dif;
+    for (int new_num_down = std::abs(num_down - down_dif); new_num_down <= num_down + down_dif; new_num_down += 2) {
+      const int bs_idx = find_bs(basis, new_num_up, new_num_down);
+      if (bs_idx < 0) continue;
+      SubBlock s;
+      s.num_up = num_up;
+      s.num_down = num_down;
+      s.down_dif = new_num_down - num_down;
+      s.row_dim = basis.sub[bs_idx].dim;
+      s.sdim = basis.sub[i].dim;
+      s.mat.assign((size_t)s.row_dim * s.sdim, czero);
+      for (int mid_num_down = std::abs(num_down - K2); mid_num_down <= num_down + K2; mid_num_down += 2) {
+        const int idx2 = find_blk3(o2, num_up, num_down, mid_num_down - num_down);
+        const int idx1 = find_blk3(o1, num_up + up_dif2, mid_num_down, new_num_down - mid_num_down);
+        if (idx1 < 0 || idx2 < 0) continue;
+        const int kq = new_num_down - num_down;   // j5 = -j4 - j6 of the normalising 3j
+        const double c11 = w3js(new_num_down, down_dif, num_down, -new_num_down, kq, num_down);
+        if (c11 == 0.0) throw std::runtime_error("block_mul_ndia: vanishing 3j normalisation");
+        double c1 = 0.0;
+        for (int m6 = -mid_num_down; m6 <= mid_num_down; m6 += 2) {
+          const int m5 = new_num_down - m6;
+          double c12 = w3js(new_num_down, K1, mid_num_down, -new_num_down, m5, m6);
+          const int m44 = -m6, m55 = -m44 - num_down;
+          c12 *= w3js(mid_num_down, K2, num_down, m44, m55, num_down) * pm1((mid_num_down + m44) / 2);
+          c12 *= w3js(K1, K2, down_dif, m5, m55, -kq) * pm1((-K1 + K2 + kq) / 2) * std::sqrt(down_dif + 1.0);
+          c1 += c12;
+        }
+        if (c1 == 0.0) continue;
         const SubBlock& a = o1.sub[idx1];
         const SubBlock& b = o2.sub[idx2];
         zgemm('N', 'N', s.row_dim, s.sdim, a.sdim, cplx(c1 / c11, 0.0), a.mat.data(), s.row_dim, b.mat.data(),
               a.sdim, cone, s.mat.data(), s.row_dim);
       }
+      nb.dim += s.sdim;
+      nb.sub.push_back(std::move(s));
     }
-    nb.dim += s.sdim;
-    nb.sub.push_back(std::move(s));
   }
   nb.num = (int)nb.sub.size();
   return nb;
+}
+
+// block_transfer_trans (block.f90:33-64): conjugate transpose of every sub-block,
+// keyed by its row quantum numbers.
+Block block_transfer_trans(const Block& in) {
+  Block out;
+  out.len = in.len;
+  out.num = in.num;
+  out.up_dif = -in.up_dif;
+  out.down_dif = in.down_dif;
+  for (const auto& x : in.sub) {
+    SubBlock s;
+    s.num_up = x.num_up + in.up_dif;
+    s.num_down = x.num_down + x.down_dif;
+    s.down_dif = -x.down_dif;
+    s.row_dim = x.sdim;
+    s.sdim = x.row_dim;
+    s.mat.assign((size_t)s.row_dim * s.sdim, czero);
+    for (int c = 0; c < s.sdim; ++c)
+      for (int r = 0; r < s.row_dim; ++r) s.mat[(size_t)c * s.row_dim + r] = std::conj(x.mat[(size_t)r * x.row_dim + c]);
+    out.dim += s.sdim;
+    out.sub.push_back(std::move(s));
+  }
+  return out;
 }
 
 const SubBasisMap* find_piece(const BasisMap& S, int bu, int bd, int su, int sd) {
@@ -1416,26 +1443,29 @@ Block Oracle::change_oper(const Block& op, int old_idx, int new_idx, bool sys, b
   return t;
 }
 
-std::vector<cplx> Oracle::density_cor(int xi) {
+// Get_density_cor (measure.f90:2525-2681) with oper1 = oper2 = op, Flags 'B',
+// xi = xj: the row <op_xi . op_j> over the partners the reference visits.
+std::vector<cplx> Oracle::oper_cor(const Block& op, int xi) {
   const Wave& w = disk_wave;
   const int N = L.num_site, ny = L.Ny, sl = w.sys_len, el = w.env_len;
-  if (xi < 1 || xi > sl - 1) throw std::runtime_error("density_cor: the site must lie in the system block");
+  if (xi < 1 || xi > sl - 1) throw std::runtime_error("oper_cor: the site must lie in the system block");
+  const double scale = std::sqrt(1.0 + op.down_dif) * (op.down_dif == 2 ? -1.0 : 1.0);
   std::vector<cplx> out(N + 1, czero);
   // partners inside the system block: Get_sys2b + measure_sys_block
   for (int j = xi + ny; j <= sl - 1; j += ny) {
-    Block a = oper_ndia(num_elec, xi, j, true, false);
-    Block b = oper_ndia(num_elec, j, j, true, false);
-    Block p = block_mul_rank0(a, b, sys_bsm.at(j));
+    Block a = oper_ndia(op, xi, j, true, false);
+    Block b = oper_ndia(op, j, j, true, false);
+    Block p = block_mul_ndia_nn(a, b, 0, sys_bsm.at(j));
     Block q;
     auto it = sys_truns.find(j);
     if (j <= 1 || it == sys_truns.end()) q = p;
     else update_trun_dia(p, q, it->second);
     Block s = change_oper(q, j, sl - 1, true, false);
-    out[j] = measure_block(s, sys_bsm.at(sl), w, true);
+    out[j] = measure_block(s, sys_bsm.at(sl), w, true) * scale;
   }
   const int last = N - N / 6 + ny;
   if (sl > last) return out;
-  Block s1 = oper_ndia(num_elec, xi, xi, true, false);
+  Block s1 = oper_ndia(op, xi, xi, true, false);
   if (xi > 1) {
     auto it = sys_truns.find(xi);
     if (it != sys_truns.end()) {
@@ -1445,16 +1475,17 @@ std::vector<cplx> Oracle::density_cor(int xi) {
     }
   }
   Block sys_oper = change_oper(s1, xi, sl - 1, true, true);
+  const Block site_op = op.down_dif == 1 ? block_transfer_trans(op) : op;
   for (int j = sl; j <= std::min(last, N); ++j) {
     if ((j - xi) % ny != 0) continue;
     cplx v = 0.0;
     if (j == sl) {
-      v = block_site_cor(sys_oper, num_elec, sys_bsm.at(sl), w);
+      v = block_site_cor(sys_oper, site_op, sys_bsm.at(sl), w);
     } else if (j == sl + 1) {
-      v = block_env_site_cor(sys_oper, num_elec, sys_bsm.at(sl), env_bsm.at(el), w);
+      v = block_env_site_cor(sys_oper, site_op, sys_bsm.at(sl), env_bsm.at(el), w);
     } else {
       const int e = N - j + 1;
-      Block e1 = oper_ndia(num_elec, e, e, false, false);
+      Block e1 = oper_ndia(op, e, e, false, false);
       if (e > 1) {
         auto it = env_truns.find(e);
         if (it != env_truns.end()) {
@@ -1464,11 +1495,17 @@ std::vector<cplx> Oracle::density_cor(int xi) {
         }
       }
       Block env_oper = change_oper(e1, e, el - 1, false, true);
+      if (op.down_dif != 0) env_oper = block_transfer_trans(env_oper);
       v = block_env_block_cor(sys_oper, env_oper, sys_bsm.at(sl), env_bsm.at(el), w);
     }
-    out[j] = v;
+    out[j] = v * scale;
   }
   return out;
 }
+
+std::vector<cplx> Oracle::density_cor(int xi) { return oper_cor(num_elec, xi); }
+
+// main.f90:275: Get_density_cor(spin_cor, st_sd, st_sd, ..., 'B', ..., xi1, xi1)
+std::vector<cplx> Oracle::spin_cor(int xi) { return oper_cor(st_sd, xi); }
 
 }  // namespace orc

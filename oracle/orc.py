@@ -55,6 +55,8 @@ def lib():
         L.orc_measure_density.restype = i
         L.orc_density_cor.argtypes = [vp, i, ctypes.POINTER(d)]
         L.orc_density_cor.restype = i
+        L.orc_oper_cor.argtypes = [vp, i, i, ctypes.POINTER(d)]
+        L.orc_oper_cor.restype = i
         _lib = L
     return _lib
 
@@ -122,6 +124,16 @@ class Oracle:
         L = lib()
         out = np.zeros(2 * self.cfg.Nx * self.cfg.Ny, dtype=np.float64)
         n = L.orc_density_cor(self.h, int(site), out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+        if n < 0:
+            raise RuntimeError(L.orc_error(self.h).decode())
+        return out[0::2] + 1j * out[1::2]
+
+    def spin_cor(self, site):
+        """<S_site . S_j>, j = 1..Num_site, of the last ground state (Get_density_cor
+        with st_sd, main.f90:275); zero where the reference computes nothing."""
+        L = lib()
+        out = np.zeros(2 * self.cfg.Nx * self.cfg.Ny, dtype=np.float64)
+        n = L.orc_oper_cor(self.h, 1, int(site), out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
         if n < 0:
             raise RuntimeError(L.orc_error(self.h).decode())
         return out[0::2] + 1j * out[1::2]

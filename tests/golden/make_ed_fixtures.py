@@ -141,9 +141,31 @@ def tj_ground_state(Nx, Ny, t1, t2, J1, J2, sign_t=-1.0, penalty=10.0):
     # density-density correlations <n_a n_b> (row a, column b; sites a+1, b+1)
     occ = np.array([[((um | dm) >> q) & 1 for q in range(ns)] for (um, dm) in states], dtype=np.float64)
     ncor = (occ.T * p) @ occ
+    # spin-spin correlations <S_a . S_b> = <Sz_a Sz_b> + (<S+_a S-_b> + <S+_b S-_a>) / 2,
+    # diagonal 3/4 <n_a>; their sum is <S^2> = 0 for the S=0 ground state
+    vg = v[:, 0]
+    szm = np.array([[0.5 * (((um >> q) & 1) - ((dm >> q) & 1)) for q in range(ns)] for (um, dm) in states])
+    flip = np.zeros((ns, ns))
+    for k, (um, dm) in enumerate(states):
+        mm = occ_modes(um, dm)
+        for a in range(ns):
+            if not (dm >> a) & 1:
+                continue
+            for b in range(ns):
+                if a == b or not (um >> b) & 1:
+                    continue
+                # S+_a S-_b: b up -> down, then a down -> up
+                num, ndm = um ^ (1 << a) ^ (1 << b), dm ^ (1 << a) ^ (1 << b)
+                m1, sg = mm, 1.0
+                for (ann, cre) in [(2 * b, 2 * b + 1), (2 * a + 1, 2 * a)]:
+                    sg *= hop_sign(m1, ann, cre)
+                    m1 = (m1 ^ (1 << ann)) | (1 << cre)
+                flip[a, b] += float(np.real(np.conj(vg[index[(num, ndm)]]) * sg * vg[k]))
+    scor = (szm.T * p) @ szm + 0.5 * (flip + flip.T)
+    np.fill_diagonal(scor, 0.75 * np.array(dens))
     return {"Nx": Nx, "Ny": Ny, "t1": t1, "t2": t2, "J1": J1, "J2": J2, "n_sites": ns,
             "n_electrons": ne, "dim": n, "e0_S0": e - penalty * s2, "S2": s2, "sign_t": sign_t,
-            "density": dens, "density_cor": ncor.tolist()}
+            "density": dens, "density_cor": ncor.tolist(), "spin_cor": scor.tolist()}
 
 
 def main():

@@ -1,4 +1,5 @@
-"""Site densities of the oracle (measure_operator_dia restated) against exact
+"""Site densities and two-point correlations of the oracle (measure_operator_dia
+and Get_density_cor restated) against exact
 diagonalisation: <n_i> of the S=0 ground state of YC4x2 and YC4x3 with and
 without t2/J2 (tests/golden/ed_and_6j.json, make_ed_fixtures.py), DMRG keeping
 every multiplet.  Tolerance 1e-8 per site (Lanczos stops at lanzero 1e-12);
@@ -27,25 +28,27 @@ def test_density_matches_ed(case):
 
 
 @pytest.mark.parametrize("case", CASES, ids=lambda c: f"YC4x{c['Nx']}_t2{c['t2']}")
-def test_density_cor_matches_ed(case):
-    """<n_i n_j> of Get_density_cor restated, after the final half sweep to
-    5 Num_site / 6 (main.f90:205-206), against the ED correlation matrix.  Sites
-    1-4 reach all four partner kinds (inside the system block through the
-    product at the partner's length, the system site, the environment site, the
-    environment block).  Tolerance 1e-8 as for <n_i>."""
+def test_correlations_match_ed(case):
+    """<n_i n_j> and <S_i . S_j> of Get_density_cor restated (num_elec, main.f90:299;
+    st_sd, main.f90:275: rank 1, scaled by -sqrt(3) as measure.f90:2586-2587 and
+    2662-2663 do), after the final half sweep to 5 Num_site / 6 (main.f90:205-206),
+    against the ED correlation matrices.  Sites 1-4 reach all four partner kinds
+    (inside the system block through the product at the partner's length, the
+    system site, the environment site, the environment block).  Tolerance 1e-8."""
     cfg = orc.RunConfig(Nx=case["Nx"], Ny=4, t1=1.0, t2=case["t2"], J1=0.4, J2=case["J2"], kept_min=400,
                         kept_warm=400, sweeps=[400, 400], lanzero=1e-12, final_half_sweep=True)
     o = orc.Oracle(cfg)
     o.run()
-    ed = np.array(case["density_cor"])
     n = case["n_sites"]
-    for site in (1, 2, 3, 4):
-        row = o.density_cor(site)
-        partners = [j for j in range(site + 4, n + 1, 4)]
-        assert partners, "no partner on the leg"
-        for j in range(1, n + 1):
-            if j in partners:
-                assert abs(row[j - 1].real - ed[site - 1, j - 1]) <= 1e-8, (site, j)
-                assert abs(row[j - 1].imag) <= 1e-12
-            else:
-                assert row[j - 1] == 0
+    for name, get in (("density_cor", o.density_cor), ("spin_cor", o.spin_cor)):
+        ed = np.array(case[name])
+        for site in (1, 2, 3, 4):
+            row = get(site)
+            partners = [j for j in range(site + 4, n + 1, 4)]
+            assert partners, "no partner on the leg"
+            for j in range(1, n + 1):
+                if j in partners:
+                    assert abs(row[j - 1].real - ed[site - 1, j - 1]) <= 1e-8, (name, site, j)
+                    assert abs(row[j - 1].imag) <= 1e-12
+                else:
+                    assert row[j - 1] == 0
