@@ -152,13 +152,15 @@ class Oracle {
   std::vector<cplx> density_cor(int site);
   // The same with oper1 = oper2 = st_sd (main.f90:275): <S_site . S_j>.
   std::vector<cplx> spin_cor(int site);
-  // Get_density_cor for any 'B' operator (scaled by sqrt(1 + rank), negated for rank 1,
-  // measure.f90:2586-2587, 2662-2663).
-  std::vector<cplx> oper_cor(const Block& op, int site);
-  // Get_sys_oper_ndia / Get_env_oper_ndia (get_sys.f90:1536-1668), Types 'B'.
-  Block oper_ndia(const Block& st, int old_idx, int new_idx, bool sys, bool trunc);
+  // The same with oper1 = st_elec_up, oper2 = st_elec_down, Flags 'F' (main.f90:288).
+  std::vector<cplx> elec_cor(int site);
+  // Get_density_cor for any pair of site operators and Flags (scaled by
+  // sqrt(1 + rank of oper1), negated for rank 1, measure.f90:2586-2587, 2662-2663).
+  std::vector<cplx> oper_cor(const Block& op1, const Block& op2, char flags, int site);
+  // Get_sys_oper_ndia / Get_env_oper_ndia (get_sys.f90:1536-1668), Types = flags.
+  Block oper_ndia(const Block& st, int old_idx, int new_idx, bool sys, bool trunc, char flags = 'B');
   // Change_sys/env_oper_ndia (get_sys.f90:1672-1778) or _dia (get_sys.f90:1281-1331), Truns.
-  Block change_oper(const Block& op, int old_idx, int new_idx, bool sys, bool ndia);
+  Block change_oper(const Block& op, int old_idx, int new_idx, bool sys, bool ndia, char flags = 'B');
 
   // hot-path entry points restated (used directly by parity tests)
   void model_wave(Model& sys, Model& env, const Basis& sys_bs, const Basis& env_bs,

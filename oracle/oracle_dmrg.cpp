@@ -1240,8 +1240,12 @@ int find_wave(const Wave& w, int su, int sd, int eu, int ed) {
   return -1;
 }
 
-// sys_block_site_cor_ndia (measure.f90:4064-4218), FlagSign 'B'
-cplx block_site_cor(const Block& bl, const Block& st, const Basis& bs, const Wave& w) {
+// sign of the electron-number parity term of the correlators: 'B' always +1,
+// 'F' (-1)^tot_num (measure.f90:4167-4178, 4830-4841, 4569-4580)
+inline double flag_sign(char flag, int tot_num) { return flag == 'F' && (tot_num % 2) ? -1.0 : 1.0; }
+
+// sys_block_site_cor_ndia (measure.f90:4064-4218)
+cplx block_site_cor(const Block& bl, const Block& st, const Basis& bs, const Wave& w, char flag) {
   const int K = bl.down_dif, up_dif = bl.up_dif;
   cplx value = 0.0;
   std::vector<cplx> mid;
@@ -1260,7 +1264,7 @@ cplx block_site_cor(const Block& bl, const Block& st, const Basis& bs, const Wav
           double c = 1.0 / std::sqrt(1.0 + K) * w6js(nbd, p.bl_num_down, K, p.st_num_down, nsd, ws.sys_num_down);
           if (c == 0.0) continue;
           c *= pm1((p.bl_num_down + nsd + K + ws.sys_num_down) / 2);
-          const cplx coef = st.sub[sid].mat[0] * c;
+          const cplx coef = flag_sign(flag, p.bl_num_up) * st.sub[sid].mat[0] * c;
           mid.assign((size_t)q->sdim * ws.env_dim, czero);
           zgemm('N', 'N', q->sdim, ws.env_dim, p.sdim, coef, bl.sub[bid].mat.data(), q->sdim, ws.vec.data() + p.spos,
                 ws.sys_dim, czero, mid.data(), q->sdim);
@@ -1272,8 +1276,9 @@ cplx block_site_cor(const Block& bl, const Block& st, const Basis& bs, const Wav
   return value;
 }
 
-// sys_block_env_site_cor_ndia (measure.f90:4666-4903), FlagSign 'B'
-cplx block_env_site_cor(const Block& bl, const Block& est, const Basis& sbs, const Basis& ebs, const Wave& w) {
+// sys_block_env_site_cor_ndia (measure.f90:4666-4903)
+cplx block_env_site_cor(const Block& bl, const Block& est, const Basis& sbs, const Basis& ebs, const Wave& w,
+                        char flag) {
   const int K = bl.down_dif, Ke = est.down_dif, up_dif = bl.up_dif;
   cplx value = 0.0;
   std::vector<cplx> mat;
@@ -1310,7 +1315,7 @@ cplx block_env_site_cor(const Block& bl, const Block& est, const Basis& sbs, con
               if ((((nsbd + x.st_num_down + ws.sys_num_down + K) / 2 + (y.bl_num_down + y.st_num_down + nend + K) / 2) %
                    2) != 0)
                 c = -c;
-              const cplx coef = est.sub[env_id].mat[0] * c;
+              const cplx coef = flag_sign(flag, ws.sys_num_up) * est.sub[env_id].mat[0] * c;
               mat.assign((size_t)qs->sdim * y.sdim, czero);
               zgemm('N', 'N', qs->sdim, y.sdim, x.sdim, coef, bl.sub[sys_id].mat.data(), qs->sdim,
                     ws.vec.data() + (size_t)y.spos * ws.sys_dim + x.spos, ws.sys_dim, czero, mat.data(), qs->sdim);
@@ -1325,8 +1330,9 @@ cplx block_env_site_cor(const Block& bl, const Block& est, const Basis& sbs, con
   return value;
 }
 
-// sys_block_env_block_cor_ndia (measure.f90:4398-4661), FlagSign 'B'
-cplx block_env_block_cor(const Block& bl, const Block& ebl, const Basis& sbs, const Basis& ebs, const Wave& w) {
+// sys_block_env_block_cor_ndia (measure.f90:4398-4661)
+cplx block_env_block_cor(const Block& bl, const Block& ebl, const Basis& sbs, const Basis& ebs, const Wave& w,
+                         char flag) {
   const int K = bl.down_dif, up_dif = bl.up_dif;
   cplx value = 0.0;
   std::vector<cplx> mat1, mat2;
@@ -1357,6 +1363,7 @@ cplx block_env_block_cor(const Block& bl, const Block& ebl, const Basis& sbs, co
               if ((((nsbd + x.st_num_down + ws.sys_num_down + K) / 2 + (nebd + y.st_num_down + ws.env_num_down + K) / 2) %
                    2) == 1)
                 c = -c;
+              c *= flag_sign(flag, ws.sys_num_up + y.st_num_up);
               const SubWave& nw = w.sub[wid];
               mat1.assign((size_t)qs->sdim * y.sdim, czero);
               mat2.assign((size_t)qs->sdim * y.sdim, czero);
@@ -1377,7 +1384,7 @@ cplx block_env_block_cor(const Block& bl, const Block& ebl, const Basis& sbs, co
 
 // Get_sys_oper_ndia / Get_env_oper_ndia (get_sys.f90:1536-1668), trun_idx = 1,
 // Types 'B'; with trunc the result is truncated at the longer length (Truns).
-Block Oracle::oper_ndia(const Block& st, int old_idx, int new_idx, bool sys, bool trunc) {
+Block Oracle::oper_ndia(const Block& st, int old_idx, int new_idx, bool sys, bool trunc, char flags) {
   const auto& bsm = sys ? sys_bsm : env_bsm;
   const auto& truns = sys ? sys_truns : env_truns;
   const int trun_idx = 1;
@@ -1387,22 +1394,22 @@ Block Oracle::oper_ndia(const Block& st, int old_idx, int new_idx, bool sys, boo
     if (one <= 1) {
       cur = st;
     } else if (one <= trun_idx) {
-      update_site_ndia(st, bsm.at(one), cur, 'B', !sys);
+      update_site_ndia(st, bsm.at(one), cur, flags, !sys);
     } else {
-      update_site_ndia(st, bsm.at(one), mid, 'B', !sys);
+      update_site_ndia(st, bsm.at(one), mid, flags, !sys);
       update_trun_ndia(mid, cur, truns.at(one));
     }
     int idx = one;
     while (idx + 1 <= two - 1) {
-      update_block_ndia(cur, bsm.at(idx + 1), mid, 'B', !sys);
+      update_block_ndia(cur, bsm.at(idx + 1), mid, flags, !sys);
       idx++;
       if (idx <= trun_idx) cur = mid;
       else update_trun_ndia(mid, cur, truns.at(idx));
     }
-    update_block_ndia(cur, bsm.at(idx + 1), out, 'B', !sys);
+    update_block_ndia(cur, bsm.at(idx + 1), out, flags, !sys);
   } else {
     if (one <= 1) out = st;
-    else update_site_ndia(st, bsm.at(two), out, 'B', !sys);
+    else update_site_ndia(st, bsm.at(two), out, flags, !sys);
   }
   auto it = truns.find(two);
   if (!trunc || it == truns.end()) return out;
@@ -1413,14 +1420,14 @@ Block Oracle::oper_ndia(const Block& st, int old_idx, int new_idx, bool sys, boo
 
 // Change_sys_oper_ndia (get_sys.f90:1672-1723; ndia) or Change_sys_oper_dia
 // (get_sys.f90:1281-1331; dia), and their env twins, with Truns = .true.
-Block Oracle::change_oper(const Block& op, int old_idx, int new_idx, bool sys, bool ndia) {
+Block Oracle::change_oper(const Block& op, int old_idx, int new_idx, bool sys, bool ndia, char flags) {
   const auto& bsm = sys ? sys_bsm : env_bsm;
   const auto& truns = sys ? sys_truns : env_truns;
   const int trun_idx = 1;
   const int one = std::min(old_idx, new_idx), two = std::max(old_idx, new_idx);
   if (one == two) return op;
   auto grow = [&](const Block& b, const Basis& bs, Block& o) {
-    if (ndia) update_block_ndia(b, bs, o, 'B', !sys);
+    if (ndia) update_block_ndia(b, bs, o, flags, !sys);
     else update_block_dia(b, bs, o);
   };
   auto trun = [&](const Block& b, Block& o, const Block& t) {
@@ -1443,29 +1450,29 @@ Block Oracle::change_oper(const Block& op, int old_idx, int new_idx, bool sys, b
   return t;
 }
 
-// Get_density_cor (measure.f90:2525-2681) with oper1 = oper2 = op, Flags 'B',
-// xi = xj: the row <op_xi . op_j> over the partners the reference visits.
-std::vector<cplx> Oracle::oper_cor(const Block& op, int xi) {
+// Get_density_cor (measure.f90:2525-2681), xi = xj: the row <op1_xi op2_j>
+// over the partners the reference visits, for its Flags ('B' or 'F').
+std::vector<cplx> Oracle::oper_cor(const Block& op1, const Block& op2, char flags, int xi) {
   const Wave& w = disk_wave;
   const int N = L.num_site, ny = L.Ny, sl = w.sys_len, el = w.env_len;
   if (xi < 1 || xi > sl - 1) throw std::runtime_error("oper_cor: the site must lie in the system block");
-  const double scale = std::sqrt(1.0 + op.down_dif) * (op.down_dif == 2 ? -1.0 : 1.0);
+  const double scale = std::sqrt(1.0 + op1.down_dif) * (op1.down_dif == 2 ? -1.0 : 1.0);
   std::vector<cplx> out(N + 1, czero);
   // partners inside the system block: Get_sys2b + measure_sys_block
   for (int j = xi + ny; j <= sl - 1; j += ny) {
-    Block a = oper_ndia(op, xi, j, true, false);
-    Block b = oper_ndia(op, j, j, true, false);
+    Block a = oper_ndia(op1, xi, j, true, false, flags);
+    Block b = oper_ndia(op2, j, j, true, false, flags);
     Block p = block_mul_ndia_nn(a, b, 0, sys_bsm.at(j));
     Block q;
     auto it = sys_truns.find(j);
     if (j <= 1 || it == sys_truns.end()) q = p;
     else update_trun_dia(p, q, it->second);
-    Block s = change_oper(q, j, sl - 1, true, false);
+    Block s = change_oper(q, j, sl - 1, true, false, flags);
     out[j] = measure_block(s, sys_bsm.at(sl), w, true) * scale;
   }
   const int last = N - N / 6 + ny;
   if (sl > last) return out;
-  Block s1 = oper_ndia(op, xi, xi, true, false);
+  Block s1 = oper_ndia(op1, xi, xi, true, false, flags);
   if (xi > 1) {
     auto it = sys_truns.find(xi);
     if (it != sys_truns.end()) {
@@ -1474,18 +1481,18 @@ std::vector<cplx> Oracle::oper_cor(const Block& op, int xi) {
       s1 = t;
     }
   }
-  Block sys_oper = change_oper(s1, xi, sl - 1, true, true);
-  const Block site_op = op.down_dif == 1 ? block_transfer_trans(op) : op;
+  Block sys_oper = change_oper(s1, xi, sl - 1, true, true, flags);
+  const Block site_op = op2.down_dif == 1 ? block_transfer_trans(op2) : op2;
   for (int j = sl; j <= std::min(last, N); ++j) {
     if ((j - xi) % ny != 0) continue;
     cplx v = 0.0;
     if (j == sl) {
-      v = block_site_cor(sys_oper, site_op, sys_bsm.at(sl), w);
+      v = block_site_cor(sys_oper, site_op, sys_bsm.at(sl), w, flags);
     } else if (j == sl + 1) {
-      v = block_env_site_cor(sys_oper, site_op, sys_bsm.at(sl), env_bsm.at(el), w);
+      v = block_env_site_cor(sys_oper, site_op, sys_bsm.at(sl), env_bsm.at(el), w, flags);
     } else {
       const int e = N - j + 1;
-      Block e1 = oper_ndia(op, e, e, false, false);
+      Block e1 = oper_ndia(op2, e, e, false, false, flags);
       if (e > 1) {
         auto it = env_truns.find(e);
         if (it != env_truns.end()) {
@@ -1494,18 +1501,21 @@ std::vector<cplx> Oracle::oper_cor(const Block& op, int xi) {
           e1 = t;
         }
       }
-      Block env_oper = change_oper(e1, e, el - 1, false, true);
-      if (op.down_dif != 0) env_oper = block_transfer_trans(env_oper);
-      v = block_env_block_cor(sys_oper, env_oper, sys_bsm.at(sl), env_bsm.at(el), w);
+      Block env_oper = change_oper(e1, e, el - 1, false, true, flags);
+      if (op2.down_dif != 0) env_oper = block_transfer_trans(env_oper);
+      v = block_env_block_cor(sys_oper, env_oper, sys_bsm.at(sl), env_bsm.at(el), w, flags);
     }
     out[j] = v * scale;
   }
   return out;
 }
 
-std::vector<cplx> Oracle::density_cor(int xi) { return oper_cor(num_elec, xi); }
+std::vector<cplx> Oracle::density_cor(int xi) { return oper_cor(num_elec, num_elec, 'B', xi); }
 
 // main.f90:275: Get_density_cor(spin_cor, st_sd, st_sd, ..., 'B', ..., xi1, xi1)
-std::vector<cplx> Oracle::spin_cor(int xi) { return oper_cor(st_sd, xi); }
+std::vector<cplx> Oracle::spin_cor(int xi) { return oper_cor(st_sd, st_sd, 'B', xi); }
+
+// main.f90:288: Get_density_cor(elec_cor, st_elec_up, st_elec_down, ..., 'F', ..., xi1, xi1)
+std::vector<cplx> Oracle::elec_cor(int xi) { return oper_cor(st_elec_up, st_elec_down, 'F', xi); }
 
 }  // namespace orc

@@ -560,12 +560,14 @@ int orc_oper_cor(void* hp, int kind, int site, double* out);
 // (re, im) for j = 1..num_site, zero where the reference computes nothing
 int orc_density_cor(void* hp, int site, double* out) { return orc_oper_cor(hp, 0, site, out); }
 
-// kind 0: <n_site n_j> (num_elec), kind 1: <S_site . S_j> (st_sd); 2 * num_site doubles
+// kind 0: <n_site n_j> (num_elec), 1: <S_site . S_j> (st_sd), 2: electron correlation
+// (st_elec_up, st_elec_down, 'F'); 2 * num_site doubles
 int orc_oper_cor(void* hp, int kind, int site, double* out) {
   OrcHandle* h = (OrcHandle*)hp;
   if (!h->o) return -1;
   try {
-    std::vector<orc::cplx> d = kind == 1 ? h->o->spin_cor(site) : h->o->density_cor(site);
+    std::vector<orc::cplx> d =
+        kind == 1 ? h->o->spin_cor(site) : kind == 2 ? h->o->elec_cor(site) : h->o->density_cor(site);
     for (size_t j = 1; j < d.size(); ++j) {
       out[2 * (j - 1)] = d[j].real();
       out[2 * (j - 1) + 1] = d[j].imag();

@@ -138,6 +138,17 @@ class Oracle:
             raise RuntimeError(L.orc_error(self.h).decode())
         return out[0::2] + 1j * out[1::2]
 
+    def elec_cor(self, site):
+        """Electron correlation of the last ground state (Get_density_cor with
+        st_elec_up, st_elec_down, Flags 'F', main.f90:288), j = 1..Num_site; zero
+        where the reference computes nothing."""
+        L = lib()
+        out = np.zeros(2 * self.cfg.Nx * self.cfg.Ny, dtype=np.float64)
+        n = L.orc_oper_cor(self.h, 2, int(site), out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+        if n < 0:
+            raise RuntimeError(L.orc_error(self.h).decode())
+        return out[0::2] + 1j * out[1::2]
+
     def capture(self):
         """Flat (ints, complex) serialisation of the captured superblock."""
         L = lib()

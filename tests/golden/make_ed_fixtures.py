@@ -163,9 +163,25 @@ def tj_ground_state(Nx, Ny, t1, t2, J1, J2, sign_t=-1.0, penalty=10.0):
                 flip[a, b] += float(np.real(np.conj(vg[index[(num, ndm)]]) * sg * vg[k]))
     scor = (szm.T * p) @ szm + 0.5 * (flip + flip.T)
     np.fill_diagonal(scor, 0.75 * np.array(dens))
+    # one-particle correlations G_ab = sum_s <c+_{a s} c_{b s}> (diagonal <n_a>)
+    ecor = np.zeros((ns, ns))
+    for k, (um, dm) in enumerate(states):
+        mm = occ_modes(um, dm)
+        for s, msk in ((0, um), (1, dm)):
+            for b in range(ns):
+                if not (msk >> b) & 1:
+                    continue
+                for a in range(ns):
+                    if a == b or (((um >> a) | (dm >> a)) & 1):
+                        continue
+                    sg = hop_sign(mm, 2 * b + s, 2 * a + s)
+                    nstate = (um ^ (1 << a) ^ (1 << b), dm) if s == 0 else (um, dm ^ (1 << a) ^ (1 << b))
+                    ecor[a, b] += float(np.real(np.conj(vg[index[nstate]]) * sg * vg[k]))
+    np.fill_diagonal(ecor, np.array(dens))
     return {"Nx": Nx, "Ny": Ny, "t1": t1, "t2": t2, "J1": J1, "J2": J2, "n_sites": ns,
             "n_electrons": ne, "dim": n, "e0_S0": e - penalty * s2, "S2": s2, "sign_t": sign_t,
-            "density": dens, "density_cor": ncor.tolist(), "spin_cor": scor.tolist()}
+            "density": dens, "density_cor": ncor.tolist(), "spin_cor": scor.tolist(),
+            "elec_cor": ecor.tolist()}
 
 
 def main():
