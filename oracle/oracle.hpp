@@ -87,6 +87,7 @@ struct Config {
   double lanzero_override = -1;  // >0: use this Lanczos tolerance in every phase
   uint64_t seed = 1;             // seeds the random_number stand-in
   bool final_half_sweep = false; // main.f90:205-206
+  int final_stop = 0;            // last label of that half sweep; 0: the reference's 5 Num_site / 6 - 1
 };
 
 // Per-Lanczos-step record (eigen.f90:169-173, den_mat.f90:342-350).
@@ -159,8 +160,21 @@ class Oracle {
   std::vector<cplx> oper_cor(const Block& op1, const Block& op2, char flags, int site);
   // Get_sys_oper_ndia / Get_env_oper_ndia (get_sys.f90:1536-1668), Types = flags.
   Block oper_ndia(const Block& st, int old_idx, int new_idx, bool sys, bool trunc, char flags = 'B');
-  // Change_sys/env_oper_ndia (get_sys.f90:1672-1778) or _dia (get_sys.f90:1281-1331), Truns.
-  Block change_oper(const Block& op, int old_idx, int new_idx, bool sys, bool ndia, char flags = 'B');
+  // Change_sys/env_oper_ndia (get_sys.f90:1672-1778) or _dia (get_sys.f90:1281-1331);
+  // trunc_end is their Truns argument.
+  Block change_oper(const Block& op, int old_idx, int new_idx, bool sys, bool ndia, char flags = 'B',
+                    bool trunc_end = true);
+  // Singlet pair correlations (Get_mSCOP_Operator_Cor0 with Flags 'S0',
+  // measure.f90:2683-2834, as main.f90:259-262 calls it): one record per pair
+  // of bonds (s1, s2) and (s3, s4) the reference visits, with its value.
+  struct PairRec {
+    int s1, s2, s3, s4;
+    cplx value;
+  };
+  std::vector<PairRec> pair_cor(int xc1, int xc2, int ij, int ij1);
+  Block sys_two(int idx1, int idx2);                                      // Get_sys_two
+  Block sys_two1(int idx2, int idx3, int idx4, const Block& pair);        // Get_sys_two1
+  Block env_scop(int idx1, int idx2, int new_idx, bool truns);            // Get_SCOP_Operator_Env
 
   // hot-path entry points restated (used directly by parity tests)
   void model_wave(Model& sys, Model& env, const Basis& sys_bs, const Basis& env_bs,

@@ -1420,7 +1420,8 @@ Block Oracle::oper_ndia(const Block& st, int old_idx, int new_idx, bool sys, boo
 
 // Change_sys_oper_ndia (get_sys.f90:1672-1723; ndia) or Change_sys_oper_dia
 // (get_sys.f90:1281-1331; dia), and their env twins, with Truns = .true.
-Block Oracle::change_oper(const Block& op, int old_idx, int new_idx, bool sys, bool ndia, char flags) {
+Block Oracle::change_oper(const Block& op, int old_idx, int new_idx, bool sys, bool ndia, char flags,
+                          bool trunc_end) {
   const auto& bsm = sys ? sys_bsm : env_bsm;
   const auto& truns = sys ? sys_truns : env_truns;
   const int trun_idx = 1;
@@ -1444,7 +1445,7 @@ Block Oracle::change_oper(const Block& op, int old_idx, int new_idx, bool sys, b
   }
   grow(cur, bsm.at(idx + 1), out);
   auto it = truns.find(two);
-  if (it == truns.end()) return out;
+  if (!trunc_end || it == truns.end()) return out;
   Block t;
   trun(out, t, it->second);
   return t;
@@ -1506,6 +1507,99 @@ std::vector<cplx> Oracle::oper_cor(const Block& op1, const Block& op2, char flag
       v = block_env_block_cor(sys_oper, env_oper, sys_bsm.at(sl), env_bsm.at(el), w, flags);
     }
     out[j] = v * scale;
+  }
+  return out;
+}
+
+// ---- singlet pair correlations (Get_mSCOP_Operator_Cor0, measure.f90:2683-2834) ------
+//
+// O+_ij = (c+_{i up} c+_{j down} - c+_{i down} c+_{j up}) / sqrt(2) (measure.f90:5441-5442)
+// is the rank-0 coupling of two st_elec_up, built at the longer length.
+
+// Get_sys_two (measure.f90:2837-2874): O+_{idx1 idx2} on the system block of
+// length idx2, truncated there.
+Block Oracle::sys_two(int idx1, int idx2) {
+  Block a = oper_ndia(st_elec_up, idx1, idx2, true, false, 'F');
+  Block b = oper_ndia(st_elec_up, idx2, idx2, true, false, 'F');
+  Block p = block_mul_ndia_nn(a, b, 0, sys_bsm.at(idx2));
+  auto it = sys_truns.find(idx2);
+  if (idx2 <= 1 || it == sys_truns.end()) return p;
+  Block t;
+  update_trun_ndia(p, t, it->second);
+  return t;
+}
+
+// Get_sys_two1 (measure.f90:2877-2932): the pair operator of length idx2 times
+// st_elec_down at idx3 (coupled to rank 1/2), times st_elec_down at idx4
+// (coupled to rank 0), carried to the system block of the wave.
+Block Oracle::sys_two1(int idx2, int idx3, int idx4, const Block& pair) {
+  const int sl = disk_wave.sys_len;
+  Block m = change_oper(pair, idx2, idx3, true, true, 'B', false);
+  Block c3 = oper_ndia(st_elec_down, idx3, idx3, true, false, 'F');
+  Block p3 = block_mul_ndia_nn(m, c3, 1, sys_bsm.at(idx3));
+  Block t3 = p3;
+  auto it3 = sys_truns.find(idx3);
+  if (idx3 > 1 && it3 != sys_truns.end()) update_trun_ndia(p3, t3, it3->second);
+  Block m4 = change_oper(t3, idx3, idx4, true, true, 'F', false);
+  Block c4 = oper_ndia(st_elec_down, idx4, idx4, true, false, 'F');
+  Block p4 = block_mul_ndia_nn(m4, c4, 0, sys_bsm.at(idx4));
+  Block t4 = p4;
+  auto it4 = sys_truns.find(idx4);
+  if (idx4 > 1 && it4 != sys_truns.end()) update_trun_dia(p4, t4, it4->second);
+  return change_oper(t4, idx4, sl - 1, true, false, 'B', true);
+}
+
+// Get_SCOP_Operator_Env with Flags 'S0' (measure.f90:5450-5505): O+_{idx1 idx2}
+// on the environment block of length idx2, carried to new_idx (truncated there
+// when truns).
+Block Oracle::env_scop(int idx1, int idx2, int new_idx, bool truns) {
+  Block a = oper_ndia(st_elec_up, idx1, idx2, false, false, 'F');
+  Block b = oper_ndia(st_elec_up, idx2, idx2, false, false, 'F');
+  Block p = block_mul_ndia_nn(a, b, 0, env_bsm.at(idx2));
+  Block e = p;
+  auto it = env_truns.find(idx2);
+  if (idx2 > 1 && it != env_truns.end()) update_trun_ndia(p, e, it->second);
+  return change_oper(e, idx2, new_idx, false, true, 'B', truns);
+}
+
+// Get_mSCOP_Operator_Cor0 from label 11 (the part main.f90:259-262 reaches),
+// Flags 'S0': the pair O+ on the bond (xc1, neib(xc1, ij1)) against the bonds
+// (sid3, neib(sid3, 1|3|5)) for sid3 on the leg of xc1 up to xc2, the system
+// block first, then the environment (values conjugated there as the reference
+// does).  The reference writes these to a file; here they are returned.
+std::vector<Oracle::PairRec> Oracle::pair_cor(int xc1, int xc2, int ij, int ij1) {
+  const Wave& w = disk_wave;
+  const int N = L.num_site, ny = L.Ny, sl = w.sys_len, el = w.env_len;
+  std::vector<PairRec> out;
+  const int sid1 = xc1, sid2 = L.NEIB(sid1, ij1);
+  if (sid2 < 1) throw std::runtime_error("pair_cor: the first bond leaves the lattice");
+  const int lo = std::min(sid1, sid2), hi = std::max(sid1, sid2);
+  if (hi > sl - 1) throw std::runtime_error("pair_cor: the first bond must lie in the system block");
+  Block pair = sys_two(lo, hi);
+  for (int sid3 = sid1 + ny + ij; sid3 <= sl - 1; sid3 += ny) {
+    if (sid3 <= hi || sid3 > xc2) continue;
+    for (int i = 1; i <= 5; i += 2) {
+      const int sid4 = L.NEIB(sid3, i);
+      if (std::min(sid4, sid3) <= hi) continue;
+      if (std::max(sid3, sid4) > sl - 1) continue;
+      Block four = sys_two1(hi, std::min(sid3, sid4), std::max(sid3, sid4), pair);
+      out.push_back(PairRec{sid1, sid2, sid3, sid4, measure_block(four, sys_bsm.at(sl), w, true)});
+    }
+  }
+  Block sys_oper = change_oper(pair, hi, sl - 1, true, true, 'B', true);
+  const int m0 = (sl + 2) % ny, m1 = (sid1 - 1) % ny;
+  for (int sid3 = sl + 2 - m0 + m1 + 1 + ij; sid3 <= xc2; sid3 += ny) {
+    const int eid1 = N - sid3 + 1;
+    if (eid1 > el - 1) continue;
+    for (int i = 1; i <= 5; i += 2) {
+      const int sid4 = L.NEIB(sid3, i);
+      if (sid4 < 1) continue;
+      const int eid2 = N - sid4 + 1;
+      if (std::max(eid1, eid2) > el - 1) continue;
+      Block env_oper = env_scop(std::min(eid1, eid2), std::max(eid1, eid2), el - 1, true);
+      const cplx v = block_env_block_cor(sys_oper, env_oper, sys_bsm.at(sl), env_bsm.at(el), w, 'B');
+      out.push_back(PairRec{sid1, sid2, sid3, sid4, std::conj(v)});
+    }
   }
   return out;
 }

@@ -382,7 +382,7 @@ void Oracle::run(std::vector<StepLog>* log) {
     left_to_right(idx1, N - idx1 - 1, tmp_err, log);
     right_to_left(N - idx1 - 1, idx1, tmp_err, log);
   }
-  if (cfg.final_half_sweep) left_to_right(idx1, 5 * N / 6 - 1, tmp_err, log);
+  if (cfg.final_half_sweep) left_to_right(idx1, cfg.final_stop > 0 ? cfg.final_stop : 5 * N / 6 - 1, tmp_err, log);
 }
 
 // ---- flat serialisation ---------------------------------------------------------
@@ -518,6 +518,9 @@ void* orc_new(int Nx, int Ny, double t1, double t2, double J1, double J2, int de
   return h;
 }
 
+// test knob: where the final half sweep stops (0: the reference's 5 Num_site / 6 - 1)
+void orc_set_final_stop(void* hp, int label) { ((OrcHandle*)hp)->o->cfg.final_stop = label; }
+
 void orc_free(void* hp) {
   OrcHandle* h = (OrcHandle*)hp;
   delete h->o;
@@ -555,6 +558,29 @@ int orc_measure_density(void* hp, double* out) {
 }
 
 int orc_oper_cor(void* hp, int kind, int site, double* out);
+
+// singlet pair correlations: up to maxrec records of 6 doubles (s1, s2, s3, s4, re, im);
+// returns the number of records
+int orc_pair_cor(void* hp, int xc1, int xc2, int ij, int ij1, double* out, int maxrec) {
+  OrcHandle* h = (OrcHandle*)hp;
+  if (!h->o) return -1;
+  try {
+    std::vector<orc::Oracle::PairRec> r = h->o->pair_cor(xc1, xc2, ij, ij1);
+    for (size_t k = 0; k < r.size() && (int)k < maxrec; ++k) {
+      double* o = out + 6 * k;
+      o[0] = r[k].s1;
+      o[1] = r[k].s2;
+      o[2] = r[k].s3;
+      o[3] = r[k].s4;
+      o[4] = r[k].value.real();
+      o[5] = r[k].value.imag();
+    }
+    return (int)r.size();
+  } catch (std::exception& e) {
+    h->err = e.what();
+    return -1;
+  }
+}
 
 // <n_site n_j> of the last ground state (Get_density_cor): 2 * num_site doubles
 // (re, im) for j = 1..num_site, zero where the reference computes nothing

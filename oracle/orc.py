@@ -57,6 +57,9 @@ def lib():
         L.orc_density_cor.restype = i
         L.orc_oper_cor.argtypes = [vp, i, i, ctypes.POINTER(d)]
         L.orc_oper_cor.restype = i
+        L.orc_set_final_stop.argtypes = [vp, i]
+        L.orc_pair_cor.argtypes = [vp, i, i, i, i, ctypes.POINTER(d), i]
+        L.orc_pair_cor.restype = i
         _lib = L
     return _lib
 
@@ -77,6 +80,7 @@ class RunConfig:
     lanzero: float = -1.0      # >0 overrides the reference's Lanczos tolerance schedule
     seed: int = 1
     final_half_sweep: bool = False   # main.f90:205-206: end at 5 Num_site / 6 (the measuring position)
+    final_stop: int = 0              # test knob: last label of that half sweep (0: the reference's)
 
 
 STEP_FIELDS = ["phase", "sys_len", "env_len", "e0", "iters", "num_state", "trun_err",
@@ -93,6 +97,8 @@ class Oracle:
         err = L.orc_error(self.h)
         if err:
             raise RuntimeError(err.decode())
+        if cfg.final_stop:
+            L.orc_set_final_stop(self.h, int(cfg.final_stop))
         self.cfg = cfg
 
     def __del__(self):
@@ -148,6 +154,20 @@ class Oracle:
         if n < 0:
             raise RuntimeError(L.orc_error(self.h).decode())
         return out[0::2] + 1j * out[1::2]
+
+    def pair_cor(self, xc1, xc2, ij=0, ij1=1):
+        """Singlet pair correlations of the last ground state (Get_mSCOP_Operator_Cor0,
+        Flags 'S0', measure.f90:2683-2834): [(s1, s2, s3, s4, value)] for the bond
+        (xc1, neib(xc1, ij1)) against the bonds (s3, neib(s3, 1|3|5)) the
+        reference visits."""
+        L = lib()
+        out = np.zeros(6 * 4096, dtype=np.float64)
+        n = L.orc_pair_cor(self.h, int(xc1), int(xc2), int(ij), int(ij1),
+                           out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), 4096)
+        if n < 0:
+            raise RuntimeError(L.orc_error(self.h).decode())
+        r = out[:6 * min(n, 4096)].reshape(-1, 6)
+        return [(int(a), int(b), int(c), int(e), complex(x, y)) for a, b, c, e, x, y in r]
 
     def capture(self):
         """Flat (ints, complex) serialisation of the captured superblock."""

@@ -7,7 +7,10 @@ energy of the full many-body Hamiltonian
 
     H = sum_<ij> [ -t_ij sum_s (c+_is c_js + h.c.) + J_ij (S_i.S_j - n_i n_j / 4) ]
 
-on the same lattice.  Lattice (restating dmrg_sub.f90:453-583): sites
+on the same lattice, and its ground-state measurements the reference computes
+(main.f90:259-299): site densities <n_a>, the correlation matrices <n_a n_b>,
+<S_a . S_b> and sum_s <c+_as c_bs>, and singlet pair correlations <O+_ab O_cd>
+over nearest-neighbour bonds.  Lattice (restating dmrg_sub.f90:453-583): sites
 i = (x-1)*Ny + y, periodic in y, open in x; nearest neighbours along (0,1),
 (1,0), (1,-1) carry (t1, J1); next-nearest along (1,1), (2,-1), (1,-2) carry
 (t2, J2).  Electron count from main.f90:93-99.  Run:  python make_ed_fixtures.py
@@ -178,10 +181,36 @@ def tj_ground_state(Nx, Ny, t1, t2, J1, J2, sign_t=-1.0, penalty=10.0):
                     nstate = (um ^ (1 << a) ^ (1 << b), dm) if s == 0 else (um, dm ^ (1 << a) ^ (1 << b))
                     ecor[a, b] += float(np.real(np.conj(vg[index[nstate]]) * sg * vg[k]))
     np.fill_diagonal(ecor, np.array(dens))
+    # singlet pair correlations <O+_ab O_cd> over the nearest-neighbour bonds,
+    # O+_ab = (c+_{a up} c+_{b dn} - c+_{a dn} c+_{b up}) / sqrt(2); O_cd |psi> is
+    # kept as a sparse vector of (N-2)-electron mode masks
+    def annihilate(m, mode):
+        if not (m >> mode) & 1:
+            return None, 0.0
+        return m ^ (1 << mode), (-1.0 if bin(m & ((1 << mode) - 1)).count("1") % 2 else 1.0)
+
+    bonds_nn = sorted({(min(i, j) - 1, max(i, j) - 1) for i, j in nn})
+    opsi = []
+    for (a, b) in bonds_nn:
+        w = {}
+        for k, (um, dm) in enumerate(states):
+            m = occ_modes(um, dm)
+            # O_ab = (c_{b dn} c_{a up} - c_{b up} c_{a dn}) / sqrt(2)
+            for (m1, m2, c) in ((2 * a, 2 * b + 1, 1.0), (2 * a + 1, 2 * b, -1.0)):
+                x, s1 = annihilate(m, m1)
+                if x is None:
+                    continue
+                y, s2 = annihilate(x, m2)
+                if y is None:
+                    continue
+                w[y] = w.get(y, 0.0) + c * s1 * s2 * float(np.real(vg[k])) / np.sqrt(2.0)
+        opsi.append(w)
+    pcor = [[sum(wx.get(key, 0.0) * val for key, val in wy.items()) for wy in opsi] for wx in opsi]
     return {"Nx": Nx, "Ny": Ny, "t1": t1, "t2": t2, "J1": J1, "J2": J2, "n_sites": ns,
             "n_electrons": ne, "dim": n, "e0_S0": e - penalty * s2, "S2": s2, "sign_t": sign_t,
             "density": dens, "density_cor": ncor.tolist(), "spin_cor": scor.tolist(),
-            "elec_cor": ecor.tolist()}
+            "elec_cor": ecor.tolist(), "pair_bonds": [[a + 1, b + 1] for a, b in bonds_nn],
+            "pair_cor": pcor}
 
 
 def main():

@@ -55,3 +55,37 @@ def test_correlations_match_ed(case):
                     assert abs(row[j - 1].imag) <= 1e-8
                 else:
                     assert row[j - 1] == 0
+
+
+@pytest.mark.parametrize("case", CASES, ids=lambda c: f"YC4x{c['Nx']}_t2{c['t2']}")
+def test_pair_cor_matches_ed(case):
+    """Singlet pair correlations <O+_ab O_cd>, O+_ab = (c+_{a up} c+_{b dn} -
+    c+_{a dn} c+_{b up}) / sqrt(2), of Get_mSCOP_Operator_Cor0 restated (Flags 'S0',
+    main.f90:259-262) against ED over nearest-neighbour bonds, for first bonds
+    (xc1, neib(xc1, 1|3|5)), xc1 = 1..4.  At the reference's measuring position
+    (after the final half sweep to 5 Num_site / 6) the second bonds lie in the
+    system block (Get_sys_two1); with the half sweep stopped at Num_site / 2 some
+    lie in the environment block (Get_SCOP_Operator_Env and the block-block
+    correlator).  Tolerance 1e-8."""
+    n = case["n_sites"]
+    bonds = {tuple(b): i for i, b in enumerate(case["pair_bonds"])}
+    ed = np.array(case["pair_cor"])
+    stops = [0] if case["Nx"] == 2 else [0, n // 2 - 1]
+    for stop in stops:
+        cfg = orc.RunConfig(Nx=case["Nx"], Ny=4, t1=1.0, t2=case["t2"], J1=0.4, J2=case["J2"], kept_min=400,
+                            kept_warm=400, sweeps=[400, 400], lanzero=1e-12, final_half_sweep=True, final_stop=stop)
+        o = orc.Oracle(cfg)
+        o.run()
+        recs = []
+        for xc1 in (1, 2, 3, 4):
+            for ij1 in (1, 3, 5):
+                try:
+                    recs += o.pair_cor(xc1, n, 0, ij1)
+                except RuntimeError:   # first bond outside the system block of this wave
+                    pass
+        assert recs
+        if stop:
+            assert any(max(c, d) > n // 2 + 1 for _, _, c, d, _ in recs), "no environment-block partner"
+        for a, b, c, d, v in recs:
+            ref = ed[bonds[(min(a, b), max(a, b))], bonds[(min(c, d), max(c, d))]]
+            assert abs(v.real - ref) <= 1e-8 and abs(v.imag) <= 1e-8, (stop, a, b, c, d)
