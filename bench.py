@@ -299,13 +299,13 @@ def split_leg(torch, dev, sb, steps, fp64_out):
     for _ in range(3):
         ctx.hpsi_device(psi.data_ptr(), out.data_ptr())
     torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
+    # the split form waits for each call (to read the context's status word), so its
+    # device time is the sum of the calls' own event brackets (input slicing + 2 launches)
+    ms = 0.0
     for _ in range(steps):
         ctx.hpsi_device(psi.data_ptr(), out.data_ptr())
-    e1.record(stream)
-    e1.synchronize()
-    ms = e0.elapsed_time(e1) / steps
+        ms += ctx.hpsi_stats()["device_ms"]
+    ms /= steps
     st = ctx.hpsi_stats()
     ctx.close()
     got = out.cpu().numpy()
@@ -355,6 +355,8 @@ def sweep_leg(dev):
             "seconds_per_sweep": sum(s["step_seconds"] for s in sw) / (len(SWEEP_CONFIG["sweeps"]) + 1),
             "lanczos_seconds": sum(s["lanczos_seconds"] for s in sw),
             "hpsi_seconds": sum(s["hpsi_seconds"] for s in sw),
+            "phase_seconds": {ph: sum(s[ph + "_seconds"] for s in sw)
+                              for ph in ("set", "lanczos", "truncate", "grow", "wave")},
             "lanczos_iters": int(sum(s["lanczos_iters"] for s in sw)),
             "split_iters": int(sum(s["split_iters"] for s in sw)),
             "final_e0": steps[-1]["e0"],
@@ -454,13 +456,11 @@ def config5_leg(torch, dev, zgemm_peak):
                 ctx.blocksparse_apply(x.data_ptr(), y.data_ptr(), mode)
             torch.cuda.synchronize()
             reps = 5
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            for _ in range(reps):
+            ms = 0.0
+            for _ in range(reps):   # each call's own event bracket (the split form waits per call)
                 ctx.blocksparse_apply(x.data_ptr(), y.data_ptr(), mode)
-            e1.record(stream)
-            e1.synchronize()
-            ms = e0.elapsed_time(e1) / reps
+                ms += ctx.hpsi_stats()["device_ms"]
+            ms /= reps
             res[form] = {"ms": ms, "tflops": flops / (ms * 1e-3) / 1e12,
                          "executed_tflops": xflops / (ms * 1e-3) / 1e12}
             ys[form] = y.cpu().numpy()

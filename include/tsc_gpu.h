@@ -102,7 +102,11 @@ long long tsc_superblock_dim(tsc_ctx* ctx);
 /* model_wave (get_sys.f90:6915-7393): out = H in, host complex128 buffers of
  * tsc_superblock_dim() elements (host->device and device->host copies included). */
 int tsc_hpsi(tsc_ctx* ctx, const double* in, double* out);
-/* Same on device pointers, enqueued on the context stream (no host copies). */
+/* Same on device pointers, enqueued on the context stream (no host copies).
+ * In the TSC_SPLIT_BF16 form the call also waits for its launches and reads the
+ * context's device status word: a bounded wait of the split kernel that ran out
+ * (see tsc_set_split_wait_limit) is returned as TSC_E_CUDA, the output then
+ * being incomplete. */
 int tsc_hpsi_device(tsc_ctx* ctx, const void* d_in, void* d_out);
 
 /* lanczos_memo_new (eigen.f90:4-199, levels=1): psi_inout is the start vector
@@ -142,6 +146,22 @@ int tsc_wave_transform(tsc_ctx* ctx, int dir, const int* ints, long long nints, 
  * warm-up, two half sweeps and nsweeps full sweeps, blocks resident in HBM.
  * Writes up to max_steps records; returns the number of Lanczos solves. */
 int tsc_dmrg_run(tsc_ctx* ctx, const tsc_sweep_config* sweep, tsc_step_log* log, int max_steps);
+
+/* Device memory the stored block models of tsc_dmrg_run may hold.  The
+ * reference writes every model to disk after each step and reads it back when
+ * the sweep returns (model_to_disk / block_to_disk, block.f90:1715-1900,
+ * dmrg_sub.f90:1119-1139); here models stay in HBM while the resident ones fit
+ * under this many bytes, and past it the least recently used ones move to host
+ * memory and return to the device when the sweep reads them (results are
+ * unchanged: the data round-trips exactly).  bytes < 0 (the default): 45 % of
+ * the device's memory; 0: every stored model lives in host memory between its
+ * uses. */
+int tsc_set_resident_limit(tsc_ctx* ctx, long long bytes);
+/* Spill counters of the stored models since the context was created: models
+ * moved to host memory, models brought back, bytes moved both ways and the wall
+ * seconds spent, the bytes now resident and the limit in force. */
+int tsc_spill_stats(tsc_ctx* ctx, long long* spills, long long* restores, double* bytes, double* seconds,
+                    long long* resident_bytes, long long* limit_bytes);
 
 /* <n_i> of every site in the last ground state of tsc_dmrg_run, sites 1..Nx*Ny
  * in the lattice order (measure_operator_dia with num_elec, measure.f90:3-62,
@@ -195,6 +215,21 @@ void* tsc_stream(tsc_ctx* ctx);
 #define TSC_SPLIT_BF16 1
 int tsc_set_precision(tsc_ctx* ctx, int mode, double split_tol);
 
+/* Pre-sliced operand views of the current superblock's split-precision task
+ * lists (no counterpart in the reference): bytes[0..2] and views[0..2] for the
+ * operator views (sliced once per superblock, coefficients folded in), the
+ * input-vector views (sliced on every H.psi) and the phase-1 intermediates.
+ * All zero in the FP64 form. */
+int tsc_split_views(tsc_ctx* ctx, long long* bytes, int* views);
+
+/* Poll limit of every bounded mbarrier wait in the split-precision kernel (no
+ * counterpart in the reference; default 1<<20, far above any wait of a healthy
+ * launch).  A wait that runs out sets the context's status word and the kernel
+ * returns; the next split call then reports TSC_E_CUDA and clears the word, and
+ * the context stays usable.  0 makes every wait give up at once, which tests of
+ * that error path use. */
+int tsc_set_split_wait_limit(tsc_ctx* ctx, long long polls);
+
 /* The FP64 H.psi schedule autotuner (on at creation; no counterpart in the
  * reference).  For superblocks of >= 8 GFLOP per H.psi it times candidate
  * schedules (CTA tile of output rows x columns, long term lists split into
@@ -241,12 +276,14 @@ int tsc_blocksparse_apply(tsc_ctx* ctx, const void* d_in, void* d_out, int mode)
  * reference).  For callers that cannot call cudaMalloc or any allocating
  * library routine when they need H.psi (a host that owns the whole device
  * memory budget through its own pool, an iteration that must not change the
- * allocation state).  Same result as tsc_hpsi_device, enqueued on the context
- * stream; its scratch is one fixed array of TSC_NOALLOC_SCRATCH_ELEMS complex128
- * elements (64 MiB) in device global memory, held by every GPU that loads the
- * library until exit.  Superblocks needing more scratch are rejected with
- * TSC_E_LIMIT.  The first call on a device resolves the array's address (make
- * it before any stream capture).  All calls share the array: calls that
+ * allocation state).  Same result as tsc_hpsi_device in the context's precision
+ * (TSC_FP64 enqueued on the context stream; TSC_SPLIT_BF16, like
+ * tsc_hpsi_device, also waits and reports a timed-out wait as TSC_E_CUDA); its
+ * scratch is one fixed array of TSC_NOALLOC_SCRATCH_ELEMS complex128 elements
+ * (64 MiB) in device global memory, held by every GPU that loads the library
+ * until exit.  Superblocks needing more scratch are rejected with TSC_E_LIMIT.
+ * tsc_create places the array on its device and resolves its address, so this
+ * entry changes no allocation state.  All calls share the array: calls that
  * overlap on the GPU race. */
 #define TSC_NOALLOC_SCRATCH_ELEMS 4194304LL
 int tsc_hpsi_noalloc(tsc_ctx* ctx, const void* d_in, void* d_out);

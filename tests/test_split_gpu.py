@@ -129,3 +129,28 @@ def test_split_error_against_inner_dimension():
         errs[K] = float(np.linalg.norm(y - ref) / np.linalg.norm(ref))
     assert errs[16] <= 5e-7
     assert errs[4096] <= 1e-6
+
+
+@pytest.mark.gpu
+def test_split_wait_timeout_is_reported_and_context_recovers(captured):
+    """A bounded wait of the split kernel that runs out (poll limit 0: every wait
+    gives up at once) comes back as TSC_E_CUDA from tsc_hpsi_device through the
+    context's own status word; with the default limit restored the next call on
+    the same context succeeds and matches the FP64 H.psi."""
+    import torch
+    from tsc_tri_t1t2j1j2_b200._lib import TscError
+    cap, ctx = captured
+    x = torch.from_numpy(cap["psi0"].vec.astype(np.complex128)).cuda()
+    y = torch.zeros_like(x)
+    torch.cuda.synchronize()
+    ctx.set_split_wait_limit(0)
+    try:
+        with pytest.raises(TscError) as ei:
+            ctx.hpsi_device(x.data_ptr(), y.data_ptr())
+        assert ei.value.code == -3
+        assert "bounded wait" in str(ei.value)
+    finally:
+        ctx.set_split_wait_limit(1 << 20)
+    ctx.hpsi_device(x.data_ptr(), y.data_ptr())
+    torch.cuda.synchronize()
+    assert rel(y.cpu().numpy(), cap["hpsi"].vec) <= 2e-5

@@ -19,7 +19,8 @@ EXPORTED = [
     "tsc_create", "tsc_destroy", "tsc_last_error", "tsc_tot_num_up", "tsc_superblock_set",
     "tsc_superblock_dim", "tsc_hpsi", "tsc_hpsi_device", "tsc_lanczos", "tsc_truncate",
     "tsc_renormalize", "tsc_wave_transform", "tsc_dmrg_run", "tsc_set_capture", "tsc_get_capture",
-    "tsc_hpsi_stats", "tsc_stream", "tsc_hpsi_noalloc", "tsc_set_precision",
+    "tsc_hpsi_stats", "tsc_stream", "tsc_hpsi_noalloc", "tsc_set_precision", "tsc_set_split_wait_limit",
+    "tsc_set_resident_limit", "tsc_spill_stats", "tsc_split_views",
     "tsc_blocksparse_set", "tsc_blocksparse_apply", "tsc_measure_density", "tsc_measure_density_cor", "tsc_set_autotune",
     "tsc_autotune_table", "tsc_autotune_superblock",
 ]
@@ -87,6 +88,10 @@ def load():
     L.tsc_stream.restype = c_void
     L.tsc_hpsi_noalloc.argtypes = [c_void, c_void, c_void]
     L.tsc_set_precision.argtypes = [c_void, c_int, c_double]
+    L.tsc_set_split_wait_limit.argtypes = [c_void, c_ll]
+    L.tsc_set_resident_limit.argtypes = [c_void, c_ll]
+    L.tsc_split_views.argtypes = [c_void, P(c_ll), P(c_int)]
+    L.tsc_spill_stats.argtypes = [c_void, P(c_ll), P(c_ll), P(c_double), P(c_double), P(c_ll), P(c_ll)]
     L.tsc_blocksparse_set.argtypes = [c_void, c_int, ctypes.POINTER(c_int), c_ll, ctypes.POINTER(c_double), c_ll,
                                       ctypes.POINTER(c_ll), ctypes.POINTER(c_double), ctypes.POINTER(c_double)]
     L.tsc_blocksparse_apply.argtypes = [c_void, c_void, c_void, c_int]

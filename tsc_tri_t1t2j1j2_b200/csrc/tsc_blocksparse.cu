@@ -162,6 +162,7 @@ void Engine::blocksparse_set(int nprob, const int* ints, long long nints, const 
   bs.p2s.gterms = bs.p2.gterms;
   bs.p1.upload(st);
   bs.p2.upload(st);
+  build_split_views(bs.p1s, bs.p2s, bs.sv, st);
   bs.p1s.upload_split(st);
   bs.p2s.upload_split(st);
   bs.p1.gterms.clear();
@@ -180,19 +181,19 @@ void Engine::blocksparse_apply(const double2* d_in, double2* d_out, bool split) 
   TaskList& a = split ? bs.p1s : bs.p1;
   TaskList& b = split ? bs.p2s : bs.p2;
   cuda_check(cudaEventRecord(ev0, st), "event");
+  if (split) slice_input(bs.sv, d_in, st);
   run_tasks(a, const_cast<double2*>(d_in), d_out, bs.scratch->p);
   run_tasks(b, const_cast<double2*>(d_in), d_out, bs.scratch->p);
   cuda_check(cudaEventRecord(ev1, st), "event");
   last_stats.hpsi_flops = bs.ref_flops;
-  last_stats.launches = (a.njobs > 0) + (b.njobs > 0) + (a.nreds > 0) + (b.nreds > 0);
+  last_stats.launches = (a.njobs > 0) + (b.njobs > 0) + (a.nreds > 0) + (b.nreds > 0) + (split ? 1 : 0);
 }
 
 }  // namespace tsc
 
 extern "C" int tsc_blocksparse_set(tsc_ctx* ctx, int nproblems, const int* ints, long long nints, const double* data,
                                    long long ncplx, long long* dim, double* flops, double* exec_flops) {
-  if (!ctx) return TSC_E_ARG;
-  try {
+  return guard(ctx, [&] {
     if (!ctx->eng) throw Error(TSC_E_STATE, "no engine");
     if (nproblems < 1 || !ints || nints < 4 || (ncplx > 0 && !data) || ncplx < 0)
       throw Error(TSC_E_ARG, "blocksparse: bad arguments");
@@ -200,31 +201,16 @@ extern "C" int tsc_blocksparse_set(tsc_ctx* ctx, int nproblems, const int* ints,
     if (dim) *dim = ctx->eng->bs.dim;
     if (flops) *flops = ctx->eng->bs.ref_flops;
     if (exec_flops) *exec_flops = ctx->eng->bs.p1.exec_flops + ctx->eng->bs.p2.exec_flops;
-    ctx->err.clear();
-    return TSC_OK;
-  } catch (Error& e) {
-    ctx->err = e.what();
-    return e.code;
-  } catch (std::exception& e) {
-    ctx->err = e.what();
-    return TSC_E_ARG;
-  }
+  });
 }
 
 extern "C" int tsc_blocksparse_apply(tsc_ctx* ctx, const void* d_in, void* d_out, int mode) {
-  if (!ctx) return TSC_E_ARG;
-  try {
+  return guard(ctx, [&] {
     if (!ctx->eng) throw Error(TSC_E_STATE, "no engine");
     if (!d_in || !d_out) throw Error(TSC_E_ARG, "null buffers");
     if (mode != TSC_FP64 && mode != TSC_SPLIT_BF16) throw Error(TSC_E_ARG, "unknown precision mode");
     ctx->eng->blocksparse_apply(static_cast<const double2*>(d_in), static_cast<double2*>(d_out), mode == TSC_SPLIT_BF16);
-    ctx->err.clear();
-    return TSC_OK;
-  } catch (Error& e) {
-    ctx->err = e.what();
-    return e.code;
-  } catch (std::exception& e) {
-    ctx->err = e.what();
-    return TSC_E_ARG;
-  }
+    // the split form waits for its launches and reports a wait that ran out
+    if (mode == TSC_SPLIT_BF16) ctx->eng->check_split_fault();
+  });
 }

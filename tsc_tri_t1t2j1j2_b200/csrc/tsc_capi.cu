@@ -12,23 +12,6 @@ using namespace tsc;
 
 namespace {
 
-template <class F>
-int guard(tsc_ctx* c, F&& f) {
-  if (!c) return TSC_E_ARG;
-  try {
-    if (c->eng) cudaSetDevice(c->device);
-    f();
-    c->err.clear();
-    return TSC_OK;
-  } catch (Error& e) {
-    c->err = e.what();
-    return e.code;
-  } catch (std::exception& e) {
-    c->err = e.what();
-    return TSC_E_ARG;
-  }
-}
-
 struct Reader {
   const int* ip;
   const int* iend;
@@ -155,6 +138,9 @@ int tsc_create(tsc_ctx** ctx, const tsc_model_config* cfg) {
   c->device = cfg->device;
   try {
     c->eng.reset(new Engine(cfg->Nx, cfg->Ny, cfg->t1, cfg->t2, cfg->J1, cfg->J2, cfg->delta, cfg->device));
+    // tsc_hpsi_noalloc's array is placed on the device here, when the context
+    // is created, so that entry point never makes the driver allocate
+    noalloc_scratch_address(cfg->device);
   } catch (Error& e) {
     c->err = e.what();
     *ctx = c;
@@ -217,6 +203,7 @@ int tsc_hpsi(tsc_ctx* ctx, const double* in, double* out) {
     E.hpsi(a.p, b.p);
     cuda_check(cudaMemcpyAsync(out, b.p, n * sizeof(double2), cudaMemcpyDeviceToHost, E.st), "d2h");
     cuda_check(cudaStreamSynchronize(E.st), "sync");
+    if (E.sb.p1s.split) E.check_split_fault();
   });
 }
 
@@ -225,6 +212,8 @@ int tsc_hpsi_device(tsc_ctx* ctx, const void* d_in, void* d_out) {
     if (!ctx->eng || !ctx->eng->sb.valid) throw Error(TSC_E_STATE, "no superblock set");
     if (!d_in || !d_out) throw Error(TSC_E_ARG, "null buffers");
     ctx->eng->hpsi((const double2*)d_in, (double2*)d_out);
+    // the split form waits for its launches and reports a wait that ran out
+    if (ctx->eng->sb.p1s.split) ctx->eng->check_split_fault();
   });
 }
 
@@ -389,6 +378,46 @@ int tsc_set_precision(tsc_ctx* ctx, int mode, double split_tol) {
     if (mode != TSC_FP64 && mode != TSC_SPLIT_BF16) throw Error(TSC_E_ARG, "unknown precision mode");
     ctx->eng->precision_ = mode;
     if (split_tol > 0) ctx->eng->split_tol_ = split_tol;
+  });
+}
+
+int tsc_set_split_wait_limit(tsc_ctx* ctx, long long polls) {
+  return guard(ctx, [&] {
+    if (!ctx->eng) throw Error(TSC_E_STATE, "no engine");
+    if (polls < 0) throw Error(TSC_E_ARG, "wait limit must be >= 0");
+    ctx->eng->split_wait_limit_ = polls > 0 ? polls : 0;
+  });
+}
+
+int tsc_split_views(tsc_ctx* ctx, long long* bytes, int* views) {
+  return guard(ctx, [&] {
+    if (!ctx->eng || !ctx->eng->sb.valid) throw Error(TSC_E_STATE, "no superblock set");
+    const SplitData& sd = ctx->eng->sb.sv;
+    for (int a = 0; a < 3; ++a) {
+      if (bytes) bytes[a] = sd.units[a] * (long long)SPLIT_UNIT;
+      if (views) views[a] = sd.nviews[a];
+    }
+  });
+}
+
+int tsc_set_resident_limit(tsc_ctx* ctx, long long bytes) {
+  return guard(ctx, [&] {
+    if (!ctx->eng) throw Error(TSC_E_STATE, "no engine");
+    ctx->eng->model_store().set_limit(bytes < 0 ? -1 : bytes);
+  });
+}
+
+int tsc_spill_stats(tsc_ctx* ctx, long long* spills, long long* restores, double* bytes, double* seconds,
+                    long long* resident_bytes, long long* limit_bytes) {
+  return guard(ctx, [&] {
+    if (!ctx->eng) throw Error(TSC_E_STATE, "no engine");
+    ModelStore& m = ctx->eng->model_store();
+    if (spills) *spills = m.spills;
+    if (restores) *restores = m.restores;
+    if (bytes) *bytes = m.moved_bytes;
+    if (seconds) *seconds = m.moved_seconds;
+    if (resident_bytes) *resident_bytes = m.resident_bytes();
+    if (limit_bytes) *limit_bytes = m.limit();
   });
 }
 

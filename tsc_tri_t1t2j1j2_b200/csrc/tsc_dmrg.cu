@@ -9,6 +9,8 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 
 #include <condition_variable>
@@ -167,9 +169,7 @@ void Engine::lanczos(double2* d_psi, double lanzero, int* iters, double* e0, dou
   int it1 = 0, it2 = 0, c1 = 0, c2 = 0;
   double ms1 = 0.0, ms2 = 0.0, e_split = 0.0;
   lanczos_run(d_psi, lanzero, split_tol_, true, &it1, &e_split, &ms1, &c1);
-  int fault = 0;
-  cuda_check(split_fault_flag(&fault, 1), "split fault flag");
-  if (fault) throw Error(-3, "split-precision kernel: a bounded wait ran out");
+  check_split_fault();
   // FP64 Lanczos from that vector, stopped on the Ritz residual
   // ||H psi - E psi|| <= 0.1 sqrt(lanzero) (from the tridiagonal, no extra H.psi)
   lanczos_run(d_psi, lanzero, 0.0, false, &it2, e0, &ms2, &c2, 0.1 * std::sqrt(lanzero));
@@ -1231,6 +1231,17 @@ void Engine::lanczos_step(int phase, DModel& sys, DModel& env, const Basis& sys_
   nsolve_++;
 }
 
+// Appends a step record; with TSC_PROGRESS set in the environment, also prints
+// it to stderr (long runs show their progress as they go).
+void Engine::record_step(const StepRec& rec, std::vector<StepRec>* log) {
+  if (log) log->push_back(rec);
+  static const bool progress = std::getenv("TSC_PROGRESS") != nullptr;
+  if (progress)
+    std::fprintf(stderr, "step phase %d sys %d env %d e0 %.12f iters %d (split %d) kept %d  %.2f s (lanczos %.2f, truncate %.2f, grow %.2f)\n",
+                 rec.phase, rec.sys_len, rec.env_len, rec.e0, rec.iters, rec.split_iters, rec.num_state,
+                 rec.step_seconds, rec.lanczos_seconds, rec.truncate_seconds, rec.grow_seconds);
+}
+
 void Engine::warm_up(int end_id, double trun_err, std::vector<StepRec>* log) {
   struct Flag {
     bool& f;
@@ -1240,8 +1251,8 @@ void Engine::warm_up(int end_id, double trun_err, std::vector<StepRec>* log) {
   int label = 1;
   L.setup(1, 1);
   DModel sys = site_model(), env = site_model();
-  sys_models[1] = sys;
-  env_models[1] = env;
+  models_.put(0, 1, sys);
+  models_.put(1, 1, env);
   while (label + 1 <= end_id) {
     auto t0 = std::chrono::steady_clock::now();
     Basis sys_bs = get_basis(sys.ham), env_bs = get_basis(env.ham);
@@ -1301,8 +1312,8 @@ void Engine::warm_up(int end_id, double trun_err, std::vector<StepRec>* log) {
     rec.truncate_seconds += secs(tp, tq);
     grow(1, env, env_bs, er.trun, sys.len);
     rec.grow_seconds += secs(tq, phase_clock(st));
-    sys_models[label + 1] = sys;
-    env_models[label + 1] = env;
+    models_.put(0, label + 1, sys);
+    models_.put(1, label + 1, env);
     sys_truns[label + 1] = sr.trun;
     env_truns[label + 1] = er.trun;
     sys_bsm[label + 1] = sys_bs;
@@ -1310,7 +1321,7 @@ void Engine::warm_up(int end_id, double trun_err, std::vector<StepRec>* log) {
     disk_layout = wl;
     disk_wave = psi;
     rec.step_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
-    if (log) log->push_back(rec);
+    record_step(rec, log);
     label++;
   }
 }
@@ -1318,7 +1329,7 @@ void Engine::warm_up(int end_id, double trun_err, std::vector<StepRec>* log) {
 void Engine::left_to_right(int bg_id, int end_id, double trun_err, std::vector<StepRec>* log) {
   const int N = L.num_site;
   int label = bg_id;
-  DModel sys = sys_models.at(label), env = env_models.at(N - label - 2);
+  DModel sys = models_.get(0, label), env = models_.get(1, N - label - 2);
   L.setup(sys.ham.len, env.ham.len);
   Basis sys_bs = get_basis(sys.ham), env_bs = get_basis(env.ham);
   WLayout wl = get_super(sys_bs, env_bs, tot_num_up, tot_num_down);
@@ -1333,7 +1344,7 @@ void Engine::left_to_right(int bg_id, int end_id, double trun_err, std::vector<S
       sys_bs = get_basis(sys.ham);
       env_bs = env_bsm.at(N - label - 1);
       Basis env_basis = env_bsm.at(N - label);
-      env = env_models.at(N - label - 2);
+      env = models_.get(1, N - label - 2);
       L.setup(sys.ham.len, env.ham.len);
       WLayout nl = get_super(sys_bs, env_bs, tot_num_up, tot_num_down);
       env_trun = env_truns.at(N - label - 1);
@@ -1371,11 +1382,11 @@ void Engine::left_to_right(int bg_id, int end_id, double trun_err, std::vector<S
     rec.truncate_seconds = secs(tp, tq);
     grow(0, sys, sys_bs, sys_trun, 0);
     rec.grow_seconds = secs(tq, phase_clock(st));
-    sys_models[label + 1] = sys;
+    models_.put(0, label + 1, sys);
     sys_truns[label + 1] = sys_trun;
     sys_bsm[label + 1] = sys_bs;
     rec.step_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
-    if (log) log->push_back(rec);
+    record_step(rec, log);
     label++;
     first = false;
   }
@@ -1384,7 +1395,7 @@ void Engine::left_to_right(int bg_id, int end_id, double trun_err, std::vector<S
 void Engine::right_to_left(int bg_id, int end_id, double trun_err, std::vector<StepRec>* log) {
   const int N = L.num_site;
   int label = bg_id;
-  DModel sys = sys_models.at(label - 1), env = env_models.at(N - label - 1);
+  DModel sys = models_.get(0, label - 1), env = models_.get(1, N - label - 1);
   L.setup(sys.ham.len, env.ham.len);
   Basis sys_bs = get_basis(sys.ham), env_bs = get_basis(env.ham);
   WLayout wl = get_super(sys_bs, env_bs, tot_num_up, tot_num_down);
@@ -1400,7 +1411,7 @@ void Engine::right_to_left(int bg_id, int end_id, double trun_err, std::vector<S
       Basis sys_basis = sys_bsm.at(label + 1);
       env_bs = get_basis(env.ham);
       WLayout nl = get_super(sys_bs, env_bs, tot_num_up, tot_num_down);
-      sys = sys_models.at(label - 1);
+      sys = models_.get(0, label - 1);
       L.setup(sys.ham.len, env.ham.len);
       sys_trun = sys_truns.at(label);
       DevBufP np = std::make_shared<DevBuf>((size_t)std::max<long long>(nl.dim, 1), st, false);
@@ -1437,11 +1448,11 @@ void Engine::right_to_left(int bg_id, int end_id, double trun_err, std::vector<S
     rec.truncate_seconds = secs(tp, tq);
     grow(1, env, env_bs, env_trun, sys.len + 1);
     rec.grow_seconds = secs(tq, phase_clock(st));
-    env_models[N - label] = env;
+    models_.put(1, N - label, env);
     env_truns[N - label] = env_trun;
     env_bsm[N - label] = env_bs;
     rec.step_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
-    if (log) log->push_back(rec);
+    record_step(rec, log);
     label--;
     first = false;
   }
@@ -1452,8 +1463,8 @@ void Engine::run(int kept_min, int kept_warm, const std::vector<int>& sweeps, do
   const int N = L.num_site;
   rng = seed;
   nsolve_ = 0;
-  sys_models.clear();
-  env_models.clear();
+  models_.clear();
+  models_.bind(st);
   sys_truns.clear();
   env_truns.clear();
   sys_bsm.clear();

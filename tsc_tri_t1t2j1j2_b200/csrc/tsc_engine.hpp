@@ -161,6 +161,7 @@ struct TaskList {
   long long part_elems = 0;
   double exec_flops = 0;   // flops the kernel executes
   long long nterms = 0;
+  SplitArenas arenas{};    // split lists: the arenas of their pre-sliced operand views
   int add_group(double2* abs_c, uint8_t base, long long c_off, int ld, int M, int N, int beta);
   // Packs the lists for the device.  Groups whose term list is much longer than
   // total_cost / (slots * waves) are split into contiguous term chunks, each
@@ -169,6 +170,65 @@ struct TaskList {
   // The same lists for the split-precision kernel (the host lists are kept).
   void upload_split(cudaStream_t st);
 };
+
+// Stored block models of both sides by length (the reference writes every
+// model to disk and reads it back when the sweep returns, block.f90:1715-1900,
+// dmrg_sub.f90:1119-1139).  Here models stay in HBM while the resident models
+// fit under a byte limit; past it, the least recently used ones move to host
+// memory and come back to the device when read.  A spilled model keeps its
+// descriptors; only its device buffers are released.
+class ModelStore {
+ public:
+  void put(int side, int len, const DModel& m);   // store; may spill older models
+  DModel get(int side, int len);                  // resident copy (restored if spilled)
+  bool has(int side, int len) const { return map_.count(key(side, len)) > 0; }
+  void clear() { map_.clear(); resident_ = 0; }
+  void bind(cudaStream_t st) { st_ = st; }
+  // bytes of device memory the stored models may hold; < 0: 45 % of the device
+  void set_limit(long long bytes) { limit_ = bytes; }
+  long long limit() const;
+  long long resident_bytes() const { return resident_; }
+  long long spills = 0, restores = 0;
+  double moved_bytes = 0, moved_seconds = 0;
+
+ private:
+  struct Entry {
+    DModel m;
+    std::vector<std::vector<double2>> host;   // per block (ham, then ops), when spilled
+    bool spilled = false;
+    long long bytes = 0;
+    unsigned long long tick = 0;
+  };
+  static long long key(int side, int len) { return (long long)side << 32 | (unsigned)len; }
+  void spill(Entry& e);
+  void restore(Entry& e);
+  void enforce(long long keep);
+  std::map<long long, Entry> map_;
+  cudaStream_t st_ = nullptr;
+  long long limit_ = -1;
+  long long resident_ = 0;
+  unsigned long long clock_ = 0;
+};
+
+// Pre-sliced operand views of a pair of split-precision lists (phase 1, phase 2).
+struct SplitData {
+  DevBufP fixed, in, t;      // arenas of SPLIT_UNIT-byte tiles: operators, input vector, intermediates
+  DevBufP in_lists;          // the input vector's views and tiles (sliced again on every call)
+  const SView* d_in_views = nullptr;
+  const STile* d_in_tiles = nullptr;
+  int n_in_tiles = 0;
+  SplitArenas arenas{};
+  long long units[3] = {0, 0, 0};
+  int nviews[3] = {0, 0, 0};
+};
+// Rewrites the GEMM terms of the split lists p1 (phase 1) and p2 (phase 2),
+// copies of the FP64 lists, to reference pre-sliced views: each operator
+// operand (with the term's coefficient folded in), each rectangle of the input
+// vector, each phase-1 intermediate read by phase 2.  Allocates the arenas,
+// slices the operator views, and keeps the input vector's tile list.
+void build_split_views(TaskList& p1, TaskList& p2, SplitData& sd, cudaStream_t st);
+// Slices the input vector's views of sd (before phase 1 of every call).
+void slice_input(const SplitData& sd, const double2* d_in, cudaStream_t st);
 
 struct Stats {
   double hpsi_ms = 0, hpsi_flops = 0, hpsi_bytes = 0;
@@ -201,6 +261,7 @@ class Engine {
     TaskList merge;            // hmerge axpy tasks
     TaskList p1, p2;           // H.psi phase 1 (intermediates) and phase 2 (outputs)
     TaskList p1s, p2s;         // the same, tiled for the split-precision kernel
+    SplitData sv;              // their pre-sliced operand views
     TaskList q1, q2;           // a candidate schedule being timed by the autotuner
     int tune_class = -1;       // size class of this superblock (-1: not tuned)
     int tune_cand = -1;        // candidate in q1/q2, used by the next H.psi
@@ -219,6 +280,7 @@ class Engine {
   struct BlockSparse {
     DevBufP ops, scratch;
     TaskList p1, p2, p1s, p2s;
+    SplitData sv;
     long long dim = 0;
     double ref_flops = 0;
     int nprob = 0;
@@ -330,6 +392,8 @@ class Engine {
     int sys_len = 0, env_len = 0;
   } cap;
 
+  ModelStore& model_store() { return models_; }
+
   // helpers
   void normalize(double2* d, long long n);
   double wave_norm2(const double2* d, long long n);
@@ -342,12 +406,21 @@ class Engine {
   double* d_red = nullptr;   // partials
   double* d_scal = nullptr;  // scalars: [0..255] alpha, [256..511] beta, [512..767] uv, [768..1023] uu, misc
   double* h_scal = nullptr;  // pinned mirror
+  // This context's device status word (a slot of d_scal): the split kernel sets
+  // it when one of its bounded waits runs out.  One word per context, so
+  // contexts running side by side never see each other's faults.
+  static constexpr int S_FAULT = 2040;
+  int* d_fault = nullptr;
+  long long split_wait_limit_ = SPLIT_WAIT_LIMIT;   // polls per bounded wait of the split kernel
+  // Waits for the stream, reads the status word and clears it; a set word
+  // becomes Error(TSC_E_CUDA).
+  void check_split_fault();
 
  private:
   uint64_t rng = 1;
   double rand01();
   void wave_initialize(const WLayout& wl, double2* d);
-  std::map<int, DModel> sys_models, env_models;
+  ModelStore models_;   // side 0: system models by length, side 1: environment models
   std::map<int, DBlock> sys_truns, env_truns;
   std::map<int, Basis> sys_bsm, env_bsm;
   WLayout disk_layout;
@@ -362,6 +435,7 @@ class Engine {
   void build_merge();
   void run_tasks(TaskList& tl, double2* in, double2* out, double2* scr);
   void capture_superblock(const DevBufP& psi);
+  void record_step(const StepRec& rec, std::vector<StepRec>* log);
   void warm_up(int end_id, double trun_err, std::vector<StepRec>* log);
   void left_to_right(int bg_id, int end_id, double trun_err, std::vector<StepRec>* log);
   void right_to_left(int bg_id, int end_id, double trun_err, std::vector<StepRec>* log);

@@ -2,11 +2,13 @@
 // site operators, bases and task-list packing.
 #include <algorithm>
 #include <array>
+#include <chrono>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
 #include <map>
 #include <mutex>
+#include <tuple>
 #include <unordered_map>
 #include <vector>
 
@@ -343,6 +345,7 @@ Engine::Engine(int Nx, int Ny, double t1, double t2, double J1, double J2, int d
   cuda_check(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "cudaStreamCreate");
   cuda_check(cudaEventCreate(&ev0), "cudaEventCreate");
   cuda_check(cudaEventCreate(&ev1), "cudaEventCreate");
+  models_.bind(st);
   L.init(Nx, Ny, t1, t2, J1, J2, 0);
   // site operators (dmrg_sub.f90:743-906)
   st_elec_up.up_dif = 1;
@@ -363,14 +366,25 @@ Engine::Engine(int Nx, int Ny, double t1, double t2, double J1, double J2, int d
   red_buf = std::make_shared<DevBuf>((size_t)(1 << 16) + 1024, st, true);
   d_red = reinterpret_cast<double*>(red_buf->p);
   d_scal = d_red + (1 << 16);
+  d_fault = reinterpret_cast<int*>(d_scal + S_FAULT);   // zero: red_buf is zero-filled
   cuda_check(cudaMallocHost((void**)&h_scal, 2048 * sizeof(double)), "cudaMallocHost");
+}
+
+void Engine::check_split_fault() {
+  cuda_check(cudaMemcpyAsync(h_scal + S_FAULT, d_fault, sizeof(int), cudaMemcpyDeviceToHost, st), "d2h");
+  cuda_check(cudaStreamSynchronize(st), "sync");
+  int f = 0;
+  std::memcpy(&f, h_scal + S_FAULT, sizeof(int));
+  if (!f) return;
+  cuda_check(cudaMemsetAsync(d_fault, 0, sizeof(int), st), "memset");
+  cuda_check(cudaStreamSynchronize(st), "sync");
+  throw Error(-3, "split-precision kernel: a bounded wait ran out (output incomplete)");
 }
 
 Engine::~Engine() {
   sb = Superblock();
   bs = BlockSparse();
-  sys_models.clear();
-  env_models.clear();
+  models_.clear();
   sys_truns.clear();
   env_truns.clear();
   disk_wave.reset();
@@ -508,6 +522,149 @@ int TaskList::add_group(double2* abs_c, uint8_t base, long long c_off, int ld, i
 // the autotuner (Engine::tune_*) picks among 32x32, 64x32 and 32x64 per size class.
 int default_tile() { return TILE_32x32; }
 
+// ---- split-precision form: pre-sliced operand views ----------------------------------
+namespace {
+struct ViewKey {
+  uint8_t base, op, role;
+  long long off;
+  int ld, rows, cols;
+  double ar, ai;
+  bool operator<(const ViewKey& o) const {
+    return std::tie(base, op, role, off, ld, rows, cols, ar, ai) <
+           std::tie(o.base, o.op, o.role, o.off, o.ld, o.rows, o.cols, o.ar, o.ai);
+  }
+};
+int view_tiles_along(const SView& v) {   // row tiles (A) or column tiles (B)
+  return v.role == 0 ? (v.rows + SPLIT_TILE_M - 1) / SPLIT_TILE_M : (v.cols + SPLIT_TILE_N - 1) / SPLIT_TILE_N;
+}
+long long view_units(const SView& v) { return (long long)view_tiles_along(v) * v.nks * (v.role == 0 ? 2 : 1); }
+}  // namespace
+
+void build_split_views(TaskList& p1, TaskList& p2, SplitData& sd, cudaStream_t st) {
+  sd = SplitData();
+  std::vector<SView> views[3];
+  std::map<ViewKey, int> index[3];
+  // phase-1 groups by their scratch offset: the intermediates phase 2 reads
+  std::map<long long, int> scr_group;
+  for (size_t g = 0; g < p1.groups.size(); ++g)
+    if (p1.groups[g].c_base == BASE_SCR) scr_group[p1.groups[g].c_off] = (int)g;
+  std::map<int, int> tview_of_group;
+  auto add_view = [&](int arena, const ViewKey& k) -> int {
+    auto it = index[arena].find(k);
+    if (it != index[arena].end()) return it->second;
+    SView v{};
+    v.src = k.off;
+    v.ar = k.ar;
+    v.ai = k.ai;
+    v.ld = k.ld;
+    v.rows = k.rows;
+    v.cols = k.cols;
+    v.role = k.role;
+    v.op = k.op;
+    v.from_in = arena == ARENA_IN;
+    v.nks = ((k.role == 0 ? k.cols : k.rows) + 15) / 16;
+    v.dst = sd.units[arena];
+    sd.units[arena] += view_units(v);
+    views[arena].push_back(v);
+    return index[arena][k] = (int)views[arena].size() - 1;
+  };
+  // the view of one operand of a term; returns (arena, view)
+  auto operand = [&](uint8_t base, long long off, int ld, uint8_t op, int role, int rows, int cols, double ar,
+                     double ai) -> std::pair<int, int> {
+    if (base == BASE_ABS) return {ARENA_FIXED, add_view(ARENA_FIXED, ViewKey{base, op, (uint8_t)role, off, ld, rows, cols, ar, ai})};
+    if (ar != 1.0 || ai != 0.0) throw Error(-1, "split views: coefficient on a live operand");
+    if (base == BASE_IN) return {ARENA_IN, add_view(ARENA_IN, ViewKey{base, op, (uint8_t)role, off, ld, rows, cols, 1.0, 0.0})};
+    if (base == BASE_SCR) {
+      auto it = scr_group.find(off);
+      if (it == scr_group.end() || role != 0 || op != OP_N) throw Error(-1, "split views: unexpected scratch operand");
+      GGroup& g = p1.groups[it->second];
+      if (g.M != rows || g.c_ld != ld || g.N != cols || p1.gterms[it->second].size() != 1)
+        throw Error(-1, "split views: scratch operand is not a whole phase-1 output");
+      auto tv = tview_of_group.find(it->second);
+      if (tv != tview_of_group.end()) return {ARENA_T, tv->second};
+      const int v = add_view(ARENA_T, ViewKey{base, op, 0, off, ld, rows, cols, 1.0, 0.0});
+      g.s_off = views[ARENA_T][v].dst;
+      tview_of_group[it->second] = v;
+      return {ARENA_T, v};
+    }
+    throw Error(-1, "split views: operand base");
+  };
+  for (TaskList* tl : {&p1, &p2})
+    for (size_t gi = 0; gi < tl->groups.size(); ++gi) {
+      const GGroup& g = tl->groups[gi];
+      for (GTerm& t : tl->gterms[gi]) {
+        if (t.kind != TK_GEMM || t.K <= 0) continue;
+        // the coefficient rides on the operator operand (on A when both are operators)
+        const bool fold_a = t.l_base == BASE_ABS;
+        const double aar = fold_a ? t.ar : 1.0, aai = fold_a ? t.ai : 0.0;
+        const double bar = fold_a ? 1.0 : t.ar, bai = fold_a ? 0.0 : t.ai;
+        auto A = operand(t.l_base, t.l_off, t.l_ld, t.l_op, 0, g.M, t.K, aar, aai);
+        auto B = operand(t.r_base, t.r_off, t.r_ld, t.r_op, 1, t.K, g.N, bar, bai);
+        const SView& va = views[A.first][A.second];
+        const SView& vb = views[B.first][B.second];
+        t.l_base = (uint8_t)A.first;
+        t.l_off = va.dst;
+        t.l_ld = va.nks;
+        t.r_base = (uint8_t)B.first;
+        t.r_off = vb.dst;
+        t.r_ld = vb.nks;
+        t.l_op = t.r_op = OP_N;
+        t.ar = 1.0;
+        t.ai = 0.0;
+        t.pad0 = 1;   // references pre-sliced views
+      }
+    }
+  // arenas; intermediates' tiles start zeroed (their padding is never written)
+  DevBufP* arena[3] = {&sd.fixed, &sd.in, &sd.t};
+  for (int a = 0; a < 3; ++a) {
+    const long long bytes = std::max<long long>(sd.units[a], 1) * SPLIT_UNIT;
+    *arena[a] = std::make_shared<DevBuf>((size_t)(bytes / sizeof(double2)), st, a == ARENA_T);
+    sd.arenas.a[a] = reinterpret_cast<unsigned char*>((*arena[a])->p);
+    sd.arenas.units[a] = std::max<long long>(sd.units[a], 1);
+    sd.nviews[a] = (int)views[a].size();
+  }
+  auto tiles_of = [&](const std::vector<SView>& vs) {
+    std::vector<STile> tl;
+    for (size_t v = 0; v < vs.size(); ++v)
+      for (int t = 0; t < view_tiles_along(vs[v]); ++t)
+        for (int ks = 0; ks < vs[v].nks; ++ks) tl.push_back(STile{(int)v, t, ks, 0});
+    return tl;
+  };
+  auto pack = [&](const std::vector<SView>& vs, const std::vector<STile>& tl, DevBufP& buf, const SView*& dv,
+                  const STile*& dt) {
+    const size_t bv = (vs.size() * sizeof(SView) + 255) / 256 * 256, bt = tl.size() * sizeof(STile);
+    buf = std::make_shared<DevBuf>((bv + bt + 15) / 16 + 1, st, false);
+    std::vector<char> host(bv + bt, 0);
+    if (!vs.empty()) std::memcpy(host.data(), vs.data(), vs.size() * sizeof(SView));
+    if (bt) std::memcpy(host.data() + bv, tl.data(), bt);
+    cuda_check(cudaMemcpyAsync(buf->p, host.data(), host.size(), cudaMemcpyHostToDevice, st), "split views upload");
+    dv = reinterpret_cast<const SView*>(buf->p);
+    dt = reinterpret_cast<const STile*>(reinterpret_cast<char*>(buf->p) + bv);
+    cuda_check(cudaStreamSynchronize(st), "split views sync");   // the host staging buffer goes out of scope
+  };
+  {  // operator views: sliced once, here
+    std::vector<STile> tl = tiles_of(views[ARENA_FIXED]);
+    DevBufP tmp;
+    const SView* dv = nullptr;
+    const STile* dt = nullptr;
+    pack(views[ARENA_FIXED], tl, tmp, dv, dt);
+    cuda_check(launch_slice_tiles(dv, dt, (int)tl.size(), nullptr, sd.arenas.a[ARENA_FIXED],
+                                  sd.arenas.units[ARENA_FIXED], st),
+               "slice operators");
+    cuda_check(cudaStreamSynchronize(st), "slice operators sync");
+  }
+  std::vector<STile> tin = tiles_of(views[ARENA_IN]);
+  pack(views[ARENA_IN], tin, sd.in_lists, sd.d_in_views, sd.d_in_tiles);
+  sd.n_in_tiles = (int)tin.size();
+  p1.arenas = p2.arenas = sd.arenas;
+}
+
+void slice_input(const SplitData& sd, const double2* d_in, cudaStream_t st) {
+  cuda_check(launch_slice_tiles(sd.d_in_views, sd.d_in_tiles, sd.n_in_tiles, d_in, sd.arenas.a[ARENA_IN],
+                                sd.arenas.units[ARENA_IN], st),
+             "slice input");
+}
+
 void TaskList::upload_split(cudaStream_t st) {
   split = true;
   upload(st, 148 * 2, 4);
@@ -624,7 +781,9 @@ void Engine::run_tasks(TaskList& tl, double2* in, double2* out, double2* scr) {
   b.p[3] = scr;
   b.part = tl.part ? tl.part->p : nullptr;
   if (tl.split)
-    cuda_check(launch_grouped_zgemm_split(tl.d_jobs, tl.njobs, tl.d_groups, tl.d_terms, b, st), "grouped_zgemm_split");
+    cuda_check(launch_grouped_zgemm_split(tl.d_jobs, tl.njobs, tl.d_groups, tl.d_terms, b, tl.arenas, d_fault,
+                                          split_wait_limit_, st),
+               "grouped_zgemm_split");
   else
     cuda_check(launch_grouped_zgemm(tl.d_jobs, tl.njobs, tl.d_groups, tl.d_terms, b, st, tl.tile), "grouped_zgemm");
   if (tl.nreds)
@@ -673,6 +832,118 @@ void Engine::download_block(const DBlock& b, std::vector<int>& ints, std::vector
     d0 += n;
   }
   cuda_check(cudaStreamSynchronize(st), "download sync");
+}
+
+// ---- stored models: device-resident under a byte limit, host memory beyond it ----
+namespace {
+template <class F>
+void for_blocks(DModel& m, F&& f) {
+  f(m.ham);
+  for (auto& os : m.sub)
+    for (auto& b : os.op) f(b);
+}
+long long model_bytes(DModel& m) {
+  long long n = 0;
+  for_blocks(m, [&](DBlock& b) {
+    if (b.buf) n += (long long)b.buf->n * (long long)sizeof(double2);
+  });
+  return n;
+}
+}  // namespace
+
+long long ModelStore::limit() const {
+  if (limit_ >= 0) return limit_;
+  size_t fr = 0, tot = 0;
+  if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) {
+    cudaGetLastError();
+    return 1ll << 62;
+  }
+  return (long long)(0.45 * (double)tot);
+}
+
+void ModelStore::spill(Entry& e) {
+  if (e.spilled) return;
+  auto t0 = std::chrono::steady_clock::now();
+  e.host.clear();
+  for_blocks(e.m, [&](DBlock& b) {
+    e.host.emplace_back();
+    if (!b.buf) return;
+    auto& h = e.host.back();
+    h.resize(b.buf->n);
+    if (b.buf->n)
+      cuda_check(cudaMemcpyAsync(h.data(), b.buf->p, b.buf->n * sizeof(double2), cudaMemcpyDeviceToHost, st_),
+                 "spill d2h");
+  });
+  cuda_check(cudaStreamSynchronize(st_), "spill sync");
+  for_blocks(e.m, [&](DBlock& b) { b.buf.reset(); });
+  e.spilled = true;
+  resident_ -= e.bytes;
+  spills++;
+  moved_bytes += (double)e.bytes;
+  moved_seconds += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+}
+
+void ModelStore::restore(Entry& e) {
+  if (!e.spilled) return;
+  auto t0 = std::chrono::steady_clock::now();
+  size_t k = 0;
+  for_blocks(e.m, [&](DBlock& b) {
+    auto& h = e.host[k++];
+    if (h.empty()) return;
+    b.buf = std::make_shared<DevBuf>(h.size(), st_, false);
+    cuda_check(cudaMemcpyAsync(b.buf->p, h.data(), h.size() * sizeof(double2), cudaMemcpyHostToDevice, st_),
+               "restore h2d");
+  });
+  cuda_check(cudaStreamSynchronize(st_), "restore sync");
+  e.host.clear();
+  e.host.shrink_to_fit();
+  e.spilled = false;
+  resident_ += e.bytes;
+  restores++;
+  moved_bytes += (double)e.bytes;
+  moved_seconds += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+}
+
+// spills least recently used models (never `keep`) until the resident ones fit
+void ModelStore::enforce(long long keep) {
+  const long long lim = limit();
+  while (resident_ > lim) {
+    Entry* victim = nullptr;
+    for (auto& kv : map_)
+      if (kv.first != keep && !kv.second.spilled && kv.second.bytes > 0 &&
+          (!victim || kv.second.tick < victim->tick))
+        victim = &kv.second;
+    if (!victim) break;
+    spill(*victim);
+  }
+}
+
+void ModelStore::put(int side, int len, const DModel& m) {
+  const long long k = key(side, len);
+  auto it = map_.find(k);
+  if (it != map_.end() && !it->second.spilled) resident_ -= it->second.bytes;
+  Entry& e = map_[k];
+  e.m = m;
+  e.host.clear();
+  e.spilled = false;
+  e.bytes = model_bytes(e.m);
+  e.tick = ++clock_;
+  resident_ += e.bytes;
+  enforce(k);
+}
+
+DModel ModelStore::get(int side, int len) {
+  const long long k = key(side, len);
+  auto it = map_.find(k);
+  if (it == map_.end()) throw Error(-4, "stored model not found (side " + std::to_string(side) + ", length " +
+                                            std::to_string(len) + ")");
+  Entry& e = it->second;
+  e.tick = ++clock_;
+  if (e.spilled) {
+    restore(e);
+    enforce(k);
+  }
+  return e.m;
 }
 
 DBlock Engine::copy_block(const DBlock& b) {

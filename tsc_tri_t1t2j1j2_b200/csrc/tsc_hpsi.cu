@@ -978,6 +978,7 @@ void Engine::build_hpsi_tasks() {
     S.p1s.gterms = S.p1.gterms;
     S.p2s.groups = S.p2.groups;
     S.p2s.gterms = S.p2.gterms;
+    build_split_views(S.p1s, S.p2s, S.sv, st);
     S.p1s.upload_split(st);
     S.p2s.upload_split(st);
     S.p1s.gterms.clear();
@@ -1123,11 +1124,12 @@ void Engine::hpsi_form(const double2* d_in, double2* d_out, bool split) {
     cuda_check(cudaEventRecord(tune_ev_[0], st), "event");
   }
   cuda_check(cudaEventRecord(ev0, st), "event");
+  if (split) slice_input(sb.sv, d_in, st);
   run_tasks(a, const_cast<double2*>(d_in), d_out, sb.scratch->p);
   run_tasks(b, const_cast<double2*>(d_in), d_out, sb.scratch->p);
   cuda_check(cudaEventRecord(ev1, st), "event");
   if (probe) cuda_check(cudaEventRecord(tune_ev_[1], st), "event");
-  last_stats.launches = (a.njobs > 0) + (b.njobs > 0) + (a.nreds > 0) + (b.nreds > 0);
+  last_stats.launches = (a.njobs > 0) + (b.njobs > 0) + (a.nreds > 0) + (b.nreds > 0) + (split ? 1 : 0);
   last_stats.hpsi_flops = sb.ref_flops;
 }
 

@@ -1,9 +1,10 @@
 // B200 (sm_100a) kernels of the superblock engine.
 //
 // grouped_zgemm: output-stationary grouped complex-FP64 GEMM.  Every job is a
-// 64x64 tile of one output group; the CTA sums all terms of the group in
-// registers (DMMA m8n8k4.f64 warp tiles, 4 real MMAs per complex product, alpha
-// folded into the B fragments) and writes the tile once: no atomics, the result
+// tile (32x32 .. 64x64) of one output group; the CTA sums all terms of the group
+// in registers (DMMA m8n8k4.f64 warp tiles, 3 real MMAs per complex product by
+// the Gauss three-multiplication form, alpha folded into the B fragments) and
+// writes the tile once: no atomics, the result
 // does not depend on launch order.  Operand tiles are staged in shared memory by
 // 16-byte cp.async (double buffered, zero fill at the ragged edges); the conj of
 // op(.)=C is applied when fragments are read.  Shared-memory rows are padded by
@@ -123,14 +124,17 @@ grouped_zgemm_kernel(const GJob* __restrict__ jobs, const GGroup* __restrict__ g
   const int wrow = wm ? mh * 8 : 0, wcol = wn ? nh * 8 : 0;
   const int mt = wm ? mtot - mh : mh, nt = wn ? ntot - nh : nh;
 
-  double cre[MI][NI][2], cim[MI][NI][2];
+  // Complex products by the three-multiplication (Gauss) form: with
+  // T1 = Ar Br, T2 = Ai Bi, T3 = (Ar + Ai)(Br + Bi), the product is
+  // (T1 - T2) + i (T3 - T1 - T2); three DMMAs per complex multiply-add instead
+  // of four.  The sums are formed once per term (the result is assembled at the end).
+  double t1[MI][NI][2], t2[MI][NI][2], t3[MI][NI][2];
 #pragma unroll
   for (int a = 0; a < MI; ++a)
 #pragma unroll
-    for (int b = 0; b < NI; ++b) {
-      cre[a][b][0] = cre[a][b][1] = 0.0;
-      cim[a][b][0] = cim[a][b][1] = 0.0;
-    }
+    for (int b = 0; b < NI; ++b)
+#pragma unroll
+      for (int e = 0; e < 2; ++e) t1[a][b][e] = t2[a][b][e] = t3[a][b][e] = 0.0;
 
   for (int ti = job.t0; ti < job.t1; ++ti) {
     const GTerm t = terms[ti];
@@ -158,13 +162,13 @@ grouped_zgemm_kernel(const GJob* __restrict__ jobs, const GGroup* __restrict__ g
         for (int kb = 0; kb < TK / 4; ++kb) {
           if (kb * 4 >= krem) break;
           const int krow = kb * 4 + lt;
-          double ar[MI], ai[MI], nai[MI], br[NI], bi[NI];
+          double ar[MI], ai[MI], as[MI], br[NI], bi[NI], bs[NI];
 #pragma unroll
           for (int mi = 0; mi < MI; ++mi) {
             double2 v = As[krow * LDS_A + wrow + mi * 8 + lg];
             ar[mi] = v.x;
             ai[mi] = lc ? -v.y : v.y;
-            nai[mi] = -ai[mi];
+            as[mi] = ar[mi] + ai[mi];
           }
 #pragma unroll
           for (int ni = 0; ni < NI; ++ni) {
@@ -172,28 +176,24 @@ grouped_zgemm_kernel(const GJob* __restrict__ jobs, const GGroup* __restrict__ g
             double vr = v.x, vi = rc ? -v.y : v.y;
             br[ni] = t.ar * vr - t.ai * vi;
             bi[ni] = t.ar * vi + t.ai * vr;
+            bs[ni] = br[ni] + bi[ni];
           }
-          // four passes so the two updates of each accumulator are 32 MMAs apart
+          // three passes so successive updates of each accumulator are MI*NI MMAs apart
 #pragma unroll
           for (int mi = 0; mi < MI; ++mi)
 #pragma unroll
             for (int ni = 0; ni < NI; ++ni)
-              if (mi < mt && ni < nt) dmma(cre[mi][ni][0], cre[mi][ni][1], ar[mi], br[ni]);
+              if (mi < mt && ni < nt) dmma(t1[mi][ni][0], t1[mi][ni][1], ar[mi], br[ni]);
 #pragma unroll
           for (int mi = 0; mi < MI; ++mi)
 #pragma unroll
             for (int ni = 0; ni < NI; ++ni)
-              if (mi < mt && ni < nt) dmma(cim[mi][ni][0], cim[mi][ni][1], ar[mi], bi[ni]);
+              if (mi < mt && ni < nt) dmma(t2[mi][ni][0], t2[mi][ni][1], ai[mi], bi[ni]);
 #pragma unroll
           for (int mi = 0; mi < MI; ++mi)
 #pragma unroll
             for (int ni = 0; ni < NI; ++ni)
-              if (mi < mt && ni < nt) dmma(cre[mi][ni][0], cre[mi][ni][1], nai[mi], bi[ni]);
-#pragma unroll
-          for (int mi = 0; mi < MI; ++mi)
-#pragma unroll
-            for (int ni = 0; ni < NI; ++ni)
-              if (mi < mt && ni < nt) dmma(cim[mi][ni][0], cim[mi][ni][1], ai[mi], br[ni]);
+              if (mi < mt && ni < nt) dmma(t3[mi][ni][0], t3[mi][ni][1], as[mi], bs[ni]);
         }
         __syncthreads();
       }
@@ -222,8 +222,10 @@ grouped_zgemm_kernel(const GJob* __restrict__ jobs, const GGroup* __restrict__ g
               vr = 1.0;
               vi = 0.0;
             }
-            cre[mi][ni][e] += t.ar * vr - t.ai * vi;
-            cim[mi][ni][e] += t.ar * vi + t.ai * vr;
+            // adds (dr, di) to the result: dr to T1 (real part T1 - T2), di + dr to T3 (imaginary T3 - T1 - T2)
+            const double dr = t.ar * vr - t.ai * vi, di = t.ar * vi + t.ai * vr;
+            t1[mi][ni][e] += dr;
+            t3[mi][ni][e] += di + dr;
           }
     }
   }
@@ -242,7 +244,8 @@ grouped_zgemm_kernel(const GJob* __restrict__ jobs, const GGroup* __restrict__ g
         int col = n0 + wcol + ni * 8 + 2 * lt + e;
         if (mi < mt && ni < nt && row < g.M && col < g.N) {
           double2* p = C + (long long)row + (long long)col * ldc;
-          double2 v = make_double2(cre[mi][ni][e], cim[mi][ni][e]);
+          const double x1 = t1[mi][ni][e], x2 = t2[mi][ni][e];
+          double2 v = make_double2(x1 - x2, t3[mi][ni][e] - x1 - x2);
           if (acc_old) {
             double2 o = *p;
             v.x += o.x;

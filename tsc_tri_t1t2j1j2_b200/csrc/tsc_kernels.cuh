@@ -34,6 +34,10 @@ struct GGroup {
   int c_ld, M, N;
   int t0, t1;
   uint8_t c_base, beta, pad0, pad1;
+  // split-precision lists only: >= 0 when the next launch reads this group's
+  // output as an A operand; the output is then also written, sliced, into the
+  // A tiles of that view (ARENA_T, first tile at s_off units)
+  long long s_off = -1;
 };
 
 // One CTA's work: tile (tm, tn) of a group over terms [t0, t1).  part < 0 writes
@@ -60,13 +64,46 @@ constexpr int GEMM_TK = 16, GEMM_THREADS = 128;
 // tile = CTA output tile edge (64: 64x64, 2 CTAs/SM; 32: 32x32, 6 CTAs/SM)
 cudaError_t launch_grouped_zgemm(const GJob* jobs, int njobs, const GGroup* groups, const GTerm* terms,
                                  Bases bases, cudaStream_t st, int tile);
+// ---- split-precision form: operands pre-sliced into stage tiles ----------------------
+// A tile of an operand view holds six BF16 planes (3 slices x re/im) of op(X) in
+// the kernel's shared-memory stage layout: A role 128 rows x 16 k (24 KB, two
+// units), B role 16 k x 64 columns (12 KB, one unit).  Views of fixed operators
+// carry the term's coefficient and are sliced once per superblock; views of the
+// input vector are sliced once per call; phase-1 intermediates are written
+// sliced by the launch that computes them.
+constexpr int SPLIT_UNIT = 12288;
+enum SplitArena : uint8_t { ARENA_FIXED = 0, ARENA_IN = 1, ARENA_T = 2 };
+struct SView {
+  long long src;       // operator: absolute address / 16; input vector: element offset
+  long long dst;       // first tile, in SPLIT_UNIT from its arena's base
+  double ar, ai;       // coefficient folded into the slices
+  int ld, rows, cols;  // source leading dimension; op(X) is rows x cols (A: M x K, B: K x N)
+  int nks;             // tiles along K
+  uint8_t from_in, op, role, pad;   // role 0: A operand, 1: B operand
+};
+struct STile {
+  int view, t, ks, pad;   // tile (t, ks) of a view: t = row tile (A) or column tile (B)
+};
+struct SplitArenas {
+  unsigned char* a[3];
+  long long units[3];   // size of each arena in SPLIT_UNIT (tile accesses are checked against it)
+};
+// Slices the listed tiles (one CTA each) of `views` into `arena`; `in` is the
+// input vector for views with from_in set.
+cudaError_t launch_slice_tiles(const SView* views, const STile* tiles, int ntiles, const double2* in,
+                               unsigned char* arena, long long arena_units, cudaStream_t st);
 // Split-precision form of launch_grouped_zgemm (BF16 slices on tcgen05, FP32
 // accumulation in tensor memory); jobs are 128 x 64 tiles of the same groups.
+// GEMM terms of its lists reference pre-sliced views: l_base / r_base = arena,
+// l_off / r_off = the view's first tile (units), l_ld / r_ld = its tiles along K.
+// Every mbarrier wait of the kernel gives up after wait_limit polls; it then
+// sets *fault (the caller's device status word) to 1 and the CTA returns with
+// its tiles partly written.
 cudaError_t launch_grouped_zgemm_split(const GJob* jobs, int njobs, const GGroup* groups, const GTerm* terms,
-                                       Bases bases, cudaStream_t st);
-// Reads (and optionally clears) the flag the split kernel sets when one of its
-// bounded mbarrier waits runs out.
-cudaError_t split_fault_flag(int* host_flag, int clear);
+                                       Bases bases, SplitArenas arenas, int* fault, long long wait_limit,
+                                       cudaStream_t st);
+// default poll limit of the split kernel's waits (far above any wait of a healthy launch)
+constexpr long long SPLIT_WAIT_LIMIT = 1ll << 20;
 constexpr int SPLIT_TILE_M = 128, SPLIT_TILE_N = 64;
 // CTA tile codes of launch_grouped_zgemm (rows x columns of the output tile)
 constexpr int TILE_32x32 = 32, TILE_64x64 = 64, TILE_64x32 = 6432, TILE_32x64 = 3264;

@@ -12,13 +12,20 @@
 // The array is a file-scope __device__ variable: every GPU that loads this
 // library holds its 64 MiB until the process exits.  Host code may not use its
 // name as a device address (on the host it is only a stand-in symbol), so the
-// first call on each device, with that device current, resolves the address
-// with cudaGetSymbolAddress and caches it; make that first call before any
-// stream capture begins.  All calls share the array and it keeps the last
-// call's contents; nothing in it needs to start at zero (every element a call
-// reads was written earlier in the same call).  Calls that overlap on the GPU --
-// two contexts, or two streams of one device, running at the same time -- race
-// on the array.
+// address is resolved with cudaGetSymbolAddress, with the device current, once
+// per device and cached.  tsc_create does this for its device: with lazy module
+// loading (the CUDA 12 default) that first lookup is what places the array on
+// the device, so it happens when the context is created, never inside
+// tsc_hpsi_noalloc.  All calls share the array and it keeps the last call's
+// contents; nothing in it needs to start at zero (every element a call reads was
+// written earlier in the same call).  Calls that overlap on the GPU -- two
+// contexts, or two streams of one device, running at the same time -- race on
+// the array.
+//
+// The entry follows the context's precision like tsc_hpsi_device: in the split
+// form it runs the split task lists and, like tsc_hpsi_device, waits for them
+// and reads the context's status word (into pinned host memory the context
+// already holds).
 #include <algorithm>
 #include <mutex>
 
@@ -51,40 +58,42 @@ double2* scratch_address(int device) {
 
 }  // namespace
 
+double2* tsc::noalloc_scratch_address(int device) { return scratch_address(device); }
+
 extern "C" int tsc_hpsi_noalloc(tsc_ctx* ctx, const void* d_in, void* d_out) {
-  if (!ctx) return TSC_E_ARG;
-  try {
+  return guard(ctx, [&] {
     if (!ctx->eng || !ctx->eng->sb.valid) throw Error(TSC_E_STATE, "no superblock set");
     if (!d_in || !d_out) throw Error(TSC_E_ARG, "null buffers");
     Engine& E = *ctx->eng;
     Engine::Superblock& S = E.sb;
-    const long long need = S.scratch_elems + std::max(S.p1.part_elems, S.p2.part_elems);
+    const bool split = S.p1s.split;   // the context's precision, as tsc_hpsi_device
+    TaskList& a = split ? S.p1s : S.p1;
+    TaskList& b = split ? S.p2s : S.p2;
+    const long long need = S.scratch_elems + std::max(a.part_elems, b.part_elems);
     if (need > kScratchElems)
       throw Error(TSC_E_LIMIT, "tsc_hpsi_noalloc: superblock needs " + std::to_string(need) +
                                    " complex scratch elements, above the fixed maximum of " +
                                    std::to_string(kScratchElems) + " (use tsc_hpsi_device)");
-    cuda_check(cudaSetDevice(ctx->device), "cudaSetDevice");
     double2* scr = scratch_address(ctx->device);
-    Bases b;
-    b.p[0] = nullptr;
-    b.p[1] = const_cast<double2*>(static_cast<const double2*>(d_in));
-    b.p[2] = static_cast<double2*>(d_out);
-    b.p[3] = scr;                       // left products at [0, scratch_elems)
-    b.part = scr + S.scratch_elems;     // partial tiles after them (phases run in order)
-    for (TaskList* tl : {&S.p1, &S.p2}) {
-      cuda_check(launch_grouped_zgemm(tl->d_jobs, tl->njobs, tl->d_groups, tl->d_terms, b, E.st, tl->tile),
-                 "grouped_zgemm");
+    Bases bs;
+    bs.p[0] = nullptr;
+    bs.p[1] = const_cast<double2*>(static_cast<const double2*>(d_in));
+    bs.p[2] = static_cast<double2*>(d_out);
+    bs.p[3] = scr;                       // left products at [0, scratch_elems)
+    bs.part = scr + S.scratch_elems;     // partial tiles after them (phases run in order)
+    if (split) slice_input(S.sv, static_cast<const double2*>(d_in), E.st);   // into the context's arenas
+    for (TaskList* tl : {&a, &b}) {
+      if (split)
+        cuda_check(launch_grouped_zgemm_split(tl->d_jobs, tl->njobs, tl->d_groups, tl->d_terms, bs, tl->arenas,
+                                              E.d_fault, E.split_wait_limit_, E.st),
+                   "grouped_zgemm_split");
+      else
+        cuda_check(launch_grouped_zgemm(tl->d_jobs, tl->njobs, tl->d_groups, tl->d_terms, bs, E.st, tl->tile),
+                   "grouped_zgemm");
       if (tl->nreds)
-        cuda_check(launch_reduce_partials(tl->d_reds, tl->nreds, tl->d_groups, b, tl->max_red_elems, E.st),
+        cuda_check(launch_reduce_partials(tl->d_reds, tl->nreds, tl->d_groups, bs, tl->max_red_elems, E.st),
                    "reduce_partials");
     }
-    ctx->err.clear();
-    return TSC_OK;
-  } catch (Error& e) {
-    ctx->err = e.what();
-    return e.code;
-  } catch (std::exception& e) {
-    ctx->err = e.what();
-    return TSC_E_ARG;
-  }
+    if (split) E.check_split_fault();
+  });
 }

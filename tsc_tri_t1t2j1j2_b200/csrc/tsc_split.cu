@@ -16,21 +16,27 @@
 // the output in FP64.  Element terms and the write-back (beta, partial tiles)
 // are done in FP64.
 //
+// Operands arrive pre-sliced.  Every GEMM operand is a view -- an operator
+// block (with the term's coefficient folded in, sliced once per superblock), a
+// rectangle of the input vector (sliced once per call by slice_tiles_kernel),
+// or a phase-1 intermediate (sliced by the phase-1 launch's own epilogue) --
+// stored as stage tiles: six BF16 planes in the canonical K-major, no-swizzle
+// UMMA layout, A tiles 128 x 16 (24 KB), B tiles 16 x 64 (12 KB).
+//
 // Persistent and warp-specialised: one CTA per SM walks the jobs blockIdx.x,
 // +gridDim.x, ... (128 x 64 output tiles of a group over a term range, in
-// longest-first order).  12 producer warps convert the FP64 operands of one
-// K=16 step -- one 8-element chunk per thread, the next step's loads in flight
-// while the current one converts -- into the 12 BF16 planes (3 slices x re/im,
-// for A and B) of a shared-memory stage in the canonical K-major, no-swizzle
-// UMMA layout, and arrive on the stage's full barrier; one lane of the MMA warp
-// issues the step's 24 MMAs into one of two TMEM accumulators and commits them
-// to the stage's empty barrier (and, after a segment's last step, to the
+// longest-first order).  One producer lane streams the K steps, each an A and a
+// B tile brought into a shared-memory stage by two bulk asynchronous copies
+// that complete on the stage's full barrier; one lane of the MMA warp issues
+// the step's 24 MMAs into one of two TMEM accumulators and commits them to the
+// stage's empty barrier (and, after a segment's last step, to the
 // accumulator's full barrier); 4 epilogue warps drain the other accumulator
 // into the tile in FP64 (the first segment with beta and the element terms,
 // later ones adding to it) while the next segment runs.
-// Every mbarrier wait is bounded: on timeout the kernel raises a CTA abort flag
-// and a device fault flag, waits (bounded) for its own MMAs, frees its tensor
-// memory and returns.
+// Every mbarrier wait is bounded (wait_limit polls, a launch argument): on
+// timeout the kernel raises a CTA abort flag and the caller's fault word, waits
+// for its own MMAs (a fixed, longer bound: issued MMAs always complete), frees
+// its tensor memory and returns.
 #include <cuda_bf16.h>
 #include <cstdint>
 
@@ -38,24 +44,24 @@
 
 namespace tsc {
 
-__device__ int g_split_fault = 0;
-
 namespace {
 
-constexpr int SP_TM = 128, SP_TN = 64, SP_TK = 16, SP_STAGES = 4;
-constexpr int SP_PRODUCER_WARPS = 12, SP_MMA_WARP = 12, SP_EPI_WARP0 = 13;
-constexpr int SP_THREADS = (SP_PRODUCER_WARPS + 1 + 4) * 32;   // 544
+constexpr int SP_TM = 128, SP_TN = 64, SP_TK = 16, SP_STAGES = 5;
+constexpr int SP_PRODUCER_WARP = 0, SP_MMA_WARP = 1;            // warps 2..5: epilogue
+constexpr int SP_THREADS = 6 * 32;
 constexpr int A_PLANE = SP_TM * SP_TK * 2;                     // bytes of one BF16 plane of A
 constexpr int B_PLANE = SP_TN * SP_TK * 2;                     // ... of B
 constexpr int STAGE_BYTES = 6 * A_PLANE + 6 * B_PLANE;         // 36,864
 constexpr int SMEM_BYTES = SP_STAGES * STAGE_BYTES + 256;      // + mbarriers, TMEM slot, abort flag
+static_assert(6 * A_PLANE == 2 * SPLIT_UNIT && 6 * B_PLANE == SPLIT_UNIT, "stage tiles are the arena tiles");
 // Two accumulators (double buffer), each [Cr hi | Ci hi | Cr lo | Ci lo]: the
 // (0,0) slice pair alone in "hi", the five smaller pairs in "lo".  Both restart
 // every SP_SEG K steps; the epilogue adds each segment into the output in FP64,
 // so no FP32 chain in tensor memory is longer than 2 * SP_SEG MMAs (hi).
 constexpr int SP_SEG = 8;
 constexpr uint32_t TMEM_COLS = 8 * SP_TN;                      // 512: the whole of an SM's tensor memory
-constexpr long long WAIT_LIMIT = 1ll << 20;
+// polls of the final wait for the CTA's own MMAs before tensor memory is freed
+constexpr long long FIN_WAIT_LIMIT = 1ll << 24;
 
 // instruction descriptor, kind::f16: D f32, A/B bf16, both K-major, N>>3, M>>4
 constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(SP_TN >> 3) << 17) |
@@ -94,10 +100,10 @@ __device__ __forceinline__ void umma_commit(uint32_t bar) {
                : "memory");
 }
 
-// Bounded wait on an mbarrier phase; gives up early when another role of the
-// CTA has raised the abort flag.
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int* abort_flag) {
-  for (long long i = 0; i < WAIT_LIMIT; ++i) {
+// Bounded wait on an mbarrier phase (at most `limit` polls); gives up early
+// when another role of the CTA has raised the abort flag.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int* abort_flag, long long limit) {
+  for (long long i = 0; i < limit; ++i) {
     if (abort_flag && (i & 1023) == 1023 && *abort_flag) return false;
     uint32_t done;
     asm volatile(
@@ -180,120 +186,57 @@ __device__ __forceinline__ void store_chunk(unsigned char* planes, int plane_byt
 // byte offset of the chunk (row r, k-chunk kc) inside a plane
 __device__ __forceinline__ int chunk_off(int r, int kc) { return (r >> 3) * 256 + kc * 128 + (r & 7) * 16; }
 
-// Steps of one CTA: its jobs (blockIdx.x, +gridDim.x, ...), their GEMM terms and
-// K=16 steps, in the order every role walks them.  Holds only what a
-// producer's loads need.
-struct StepIter {
-  const GJob* jobs;
-  const GGroup* groups;
-  const GTerm* terms;
-  const Bases* bases;
-  int njobs, jb;          // current job (global index)
-  int t1, ti, kk, nk;     // job's term end, current term, its step, its steps
-  int m0, n0, M, N;       // tile origin and group extent
-  const double2* L;       // current term
-  const double2* R;
-  int l_ld, r_ld, K;
-  bool l_conj, l_n, r_conj, r_n;
-  double ar, ai;
-  bool valid;
-
-  __device__ bool load_term(int i) {
-    const GTerm t = terms[i];
-    if (t.kind != TK_GEMM || t.K <= 0) return false;
-    L = bases->p[t.l_base] + t.l_off;
-    R = bases->p[t.r_base] + t.r_off;
-    l_ld = t.l_ld;
-    r_ld = t.r_ld;
-    K = t.K;
-    l_n = t.l_op == OP_N;
-    l_conj = t.l_op == OP_C;
-    r_n = t.r_op == OP_N;
-    r_conj = t.r_op == OP_C;
-    ar = t.ar;
-    ai = t.ai;
-    kk = 0;
-    nk = (t.K + SP_TK - 1) / SP_TK;
-    return true;
-  }
-  __device__ void first_job(int j) {
-    valid = false;
-    for (jb = j; jb < njobs; jb += gridDim.x) {
-      const GJob job = jobs[jb];
-      const GGroup g = groups[job.group];
-      m0 = job.tm * SP_TM;
-      n0 = job.tn * SP_TN;
-      M = g.M;
-      N = g.N;
-      t1 = job.t1;
-      for (ti = job.t0; ti < t1; ++ti)
-        if (load_term(ti)) {
-          valid = true;
-          return;
-        }
-    }
-  }
-  __device__ void init(const GJob* j_, const GGroup* g_, const GTerm* t_, const Bases* b_, int n) {
-    jobs = j_;
-    groups = g_;
-    terms = t_;
-    bases = b_;
-    njobs = n;
-    first_job(blockIdx.x);
-  }
-  __device__ void next() {
-    if (++kk < nk) return;
-    for (++ti; ti < t1; ++ti)
-      if (load_term(ti)) return;
-    first_job(jb + gridDim.x);
-  }
-};
-
-// loads this thread's chunk of the current step: 8 consecutive k of one row of
-// op(L) (chunks 0..255) or of one column of op(R) (chunks 256..383), raw
-__device__ __forceinline__ void load_chunk(const StepIter& it, int chunk, double2* v) {
-  if (chunk < 256) {
-    const int r = chunk & 127, kc = chunk >> 7;
-    const int gi = it.m0 + r, kb = it.kk * SP_TK + kc * 8;
+// Pre-slices one stage tile of an operand view (the slice kernel below): the
+// tile's chunk `chunk` -- 8 consecutive k of one row of op(X) (A role, chunks
+// 0..255 of a 128 x 16 tile) or of one column (B role, chunks 0..127 of a
+// 16 x 64 tile) -- times the view's coefficient, into the tile's six planes.
+__device__ __forceinline__ void slice_chunk(const SView& v, const double2* X, int t, int ks, int chunk,
+                                            unsigned char* tile) {
+  double2 x[8];
+  const bool a_role = v.role == 0;
+  const int r = a_role ? (chunk & 127) : (chunk & 63);
+  const int kc = a_role ? (chunk >> 7) : (chunk >> 6);
+  const int g = t * (a_role ? SP_TM : SP_TN) + r;   // row (A) or column (B) of op(X)
+  const int kb = ks * SP_TK + kc * 8;
+  const int gmax = a_role ? v.rows : v.cols, kmax = a_role ? v.cols : v.rows;
 #pragma unroll
-    for (int e = 0; e < 8; ++e) {
-      const int k = kb + e;
-      double2 x = make_double2(0.0, 0.0);
-      if (gi < it.M && k < it.K)
-        x = it.l_n ? it.L[(long long)gi + (long long)k * it.l_ld] : it.L[(long long)k + (long long)gi * it.l_ld];
-      v[e] = x;
+  for (int e = 0; e < 8; ++e) {
+    const int k = kb + e;
+    double2 y = make_double2(0.0, 0.0);
+    if (g < gmax && k < kmax) {
+      // A: op(X)[g][k];  B: op(X)[k][g];  op N reads X as stored, op C its conjugate transpose
+      const long long i = a_role ? (v.op == OP_N ? (long long)g + (long long)k * v.ld : (long long)k + (long long)g * v.ld)
+                                 : (v.op == OP_N ? (long long)k + (long long)g * v.ld : (long long)g + (long long)k * v.ld);
+      y = X[i];
+      if (v.op == OP_C) y.y = -y.y;
     }
-  } else {
-    const int c = (chunk - 256) & 63, kc = (chunk - 256) >> 6;
-    const int gj = it.n0 + c, kb = it.kk * SP_TK + kc * 8;
-#pragma unroll
-    for (int e = 0; e < 8; ++e) {
-      const int k = kb + e;
-      double2 x = make_double2(0.0, 0.0);
-      if (gj < it.N && k < it.K)
-        x = it.r_n ? it.R[(long long)k + (long long)gj * it.r_ld] : it.R[(long long)gj + (long long)k * it.r_ld];
-      v[e] = x;
-    }
+    x[e] = make_double2(v.ar * y.x - v.ai * y.y, v.ar * y.y + v.ai * y.x);
   }
+  store_chunk(tile, a_role ? A_PLANE : B_PLANE, chunk_off(r, kc), x);
 }
 
-// conj / alpha of a loaded chunk, then its slices into the stage
-__device__ __forceinline__ void store_loaded(bool conj, double ar, double ai, int chunk, unsigned char* st,
-                                             double2* v) {
-  if (chunk < 256) {
-    if (conj)
-#pragma unroll
-      for (int e = 0; e < 8; ++e) v[e].y = -v[e].y;
-    store_chunk(st, A_PLANE, chunk_off(chunk & 127, chunk >> 7), v);
-  } else {
-#pragma unroll
-    for (int e = 0; e < 8; ++e) {
-      const double xr = v[e].x, xi = conj ? -v[e].y : v[e].y;
-      v[e] = make_double2(ar * xr - ai * xi, ar * xi + ai * xr);
-    }
-    const int c = (chunk - 256) & 63, kc = (chunk - 256) >> 6;
-    store_chunk(st + 6 * A_PLANE, B_PLANE, chunk_off(c, kc), v);
-  }
+__global__ void __launch_bounds__(256) slice_tiles_kernel(const SView* __restrict__ views,
+                                                          const STile* __restrict__ tiles, const double2* in,
+                                                          unsigned char* arena, long long arena_units) {
+  const STile tl = tiles[blockIdx.x];
+  const SView v = views[tl.view];
+  const double2* X = v.from_in ? in + v.src : reinterpret_cast<const double2*>((uintptr_t)v.src * sizeof(double2));
+  const long long unit = v.dst + (long long)(tl.t * v.nks + tl.ks) * (v.role == 0 ? 2 : 1);
+  if (unit < 0 || unit + (v.role == 0 ? 2 : 1) > arena_units) return;   // never outside the arena
+  unsigned char* tile = arena + unit * SPLIT_UNIT;
+  const int nchunk = v.role == 0 ? 256 : 128;
+  if ((int)threadIdx.x < nchunk) slice_chunk(v, X, tl.t, tl.ks, threadIdx.x, tile);
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint32_t bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+
+// bulk asynchronous copy global -> shared (no tensor map), completing on an mbarrier
+__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+               "l"(src), "r"(bytes), "r"(bar)
+               : "memory");
 }
 
 __device__ __forceinline__ void mbar_arrive(uint32_t bar) {
@@ -316,7 +259,8 @@ __device__ __forceinline__ int job_steps(const GJob& job, const GTerm* terms) {
 // accumulators, warps 13..16 drain the other accumulator into the outputs.
 __global__ void __launch_bounds__(SP_THREADS, 1)
 grouped_zgemm_split_kernel(const GJob* __restrict__ jobs, int njobs, const GGroup* __restrict__ groups,
-                           const GTerm* __restrict__ terms, Bases bases) {
+                           const GTerm* __restrict__ terms, Bases bases, SplitArenas arenas, int* fault,
+                           long long wait_limit) {
   extern __shared__ __align__(1024) unsigned char smem[];
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + SP_STAGES * STAGE_BYTES);
   uint64_t* empty = full + SP_STAGES;
@@ -329,7 +273,7 @@ grouped_zgemm_split_kernel(const GJob* __restrict__ jobs, int njobs, const GGrou
 
   if (tid == 0) {
     for (int s = 0; s < SP_STAGES; ++s) {
-      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&full[s])), "r"(SP_PRODUCER_WARPS) : "memory");
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&full[s])) : "memory");
       asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&empty[s])) : "memory");
     }
     for (int a = 0; a < 2; ++a) {
@@ -354,33 +298,59 @@ grouped_zgemm_split_kernel(const GJob* __restrict__ jobs, int njobs, const GGrou
 
   auto fail = [&]() {
     *abort_flag = 1;
-    atomicExch(&g_split_fault, 1);
+    atomicExch(fault, 1);
   };
 
-  if (warp < SP_PRODUCER_WARPS) {
-    // ---------------------------------------------------------------- producers
-    StepIter it;
-    it.init(jobs, groups, terms, &bases, njobs);
-    double2 nxt[8];
-    if (it.valid) load_chunk(it, tid, nxt);
-    for (int q = 0; it.valid; ++q) {
-      double2 cur[8];
+  if (warp == SP_PRODUCER_WARP) {
+    // ---------------------------------------------------------------- producer
+    // One lane streams the CTA's K steps: per step, the A tile (24 KB) and the
+    // B tile (12 KB) of the term's pre-sliced operand views, by two bulk copies
+    // that complete on the stage's full barrier.
+    if (lane == 0) {
+      int last[SP_STAGES];   // last fill issued into each stage (-1: none)
 #pragma unroll
-      for (int e = 0; e < 8; ++e) cur[e] = nxt[e];
-      const bool conj = tid < 256 ? it.l_conj : it.r_conj;
-      const double ar = it.ar, ai = it.ai;
-      const int s = q % SP_STAGES;
-      it.next();
-      if (it.valid) load_chunk(it, tid, nxt);   // in flight while this step converts
-      if (q >= SP_STAGES && !mbar_wait(smem_u32(&empty[s]), (uint32_t)((q / SP_STAGES - 1) & 1), abort_flag)) {
-        fail();
-        break;
+      for (int s = 0; s < SP_STAGES; ++s) last[s] = -1;
+      int q = 0;
+      bool ok = true;
+      for (int jb = blockIdx.x; jb < njobs && ok; jb += gridDim.x) {
+        const GJob job = jobs[jb];
+        for (int ti = job.t0; ti < job.t1 && ok; ++ti) {
+          const GTerm t = terms[ti];
+          if (t.kind != TK_GEMM || t.K <= 0) continue;
+          const int nk = (t.K + SP_TK - 1) / SP_TK;
+          // A tile (tm, kk) of the A view at units l_off + (tm * nks + kk) * 2; B tile (tn, kk) at r_off + tn * nks + kk
+          const long long ua = t.l_off + 2ll * job.tm * t.l_ld, ub = t.r_off + (long long)job.tn * t.r_ld;
+          // every tile this term will copy lies inside its arena, or the CTA stops with a fault
+          if (t.l_base > 2 || t.r_base > 2 || ua < 0 || ub < 0 || ua + 2ll * nk > arenas.units[t.l_base] ||
+              ub + nk > arenas.units[t.r_base]) {
+            ok = false;
+            break;
+          }
+          const unsigned char* A = arenas.a[t.l_base] + ua * SPLIT_UNIT;
+          const unsigned char* B = arenas.a[t.r_base] + ub * SPLIT_UNIT;
+          for (int kk = 0; kk < nk; ++kk, ++q) {
+            const int s = q % SP_STAGES;
+            if (q >= SP_STAGES &&
+                !mbar_wait(smem_u32(&empty[s]), (uint32_t)((q / SP_STAGES - 1) & 1), abort_flag, wait_limit)) {
+              ok = false;
+              break;
+            }
+            const uint32_t st0 = smem_u32(smem + s * STAGE_BYTES), fb = smem_u32(&full[s]);
+            mbar_arrive_expect_tx(fb, STAGE_BYTES);
+            bulk_g2s(st0, A + 2ll * kk * SPLIT_UNIT, 6 * A_PLANE, fb);
+            bulk_g2s(st0 + 6 * A_PLANE, B + (long long)kk * SPLIT_UNIT, 6 * B_PLANE, fb);
+            last[s] = q;
+          }
+        }
       }
-      store_loaded(conj, ar, ai, tid, smem + s * STAGE_BYTES, cur);
-      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-      __syncwarp();
-      if (lane == 0) mbar_arrive(smem_u32(&full[s]));
+      if (!ok) fail();
+      // every copy issued here has landed before the CTA leaves, consumed or not
+      for (int s = 0; s < SP_STAGES; ++s)
+        if (last[s] >= 0 &&
+            !mbar_wait(smem_u32(&full[s]), (uint32_t)((last[s] / SP_STAGES) & 1), nullptr, FIN_WAIT_LIMIT))
+          fail();
     }
+    __syncwarp();
   } else if (warp == SP_MMA_WARP) {
     // ---------------------------------------------------------------- MMA issuer
     if (lane == 0) {
@@ -392,7 +362,7 @@ grouped_zgemm_split_kernel(const GJob* __restrict__ jobs, int njobs, const GGrou
           const int si = i % SP_SEG;
           const int a = sg & 1, ua = sg >> 1;
           if (si == 0) {   // a segment starts: wait until the epilogue has drained this accumulator
-            if (ua >= 1 && !mbar_wait(smem_u32(&acce[a]), (uint32_t)((ua - 1) & 1), abort_flag)) {
+            if (ua >= 1 && !mbar_wait(smem_u32(&acce[a]), (uint32_t)((ua - 1) & 1), abort_flag, wait_limit)) {
               ok = false;
               break;
             }
@@ -400,7 +370,7 @@ grouped_zgemm_split_kernel(const GJob* __restrict__ jobs, int njobs, const GGrou
           }
           const uint32_t dhr = tmem + a * (4 * SP_TN), dhi = dhr + SP_TN, dlr = dhr + 2 * SP_TN, dli = dhr + 3 * SP_TN;
           const int s = q % SP_STAGES;
-          if (!mbar_wait(smem_u32(&full[s]), (uint32_t)((q / SP_STAGES) & 1), abort_flag)) {
+          if (!mbar_wait(smem_u32(&full[s]), (uint32_t)((q / SP_STAGES) & 1), abort_flag, wait_limit)) {
             ok = false;
             break;
           }
@@ -428,7 +398,7 @@ grouped_zgemm_split_kernel(const GJob* __restrict__ jobs, int njobs, const GGrou
       if (!ok) fail();
       // every MMA issued here has completed before the accumulators are freed
       umma_commit(smem_u32(fin));
-      if (!mbar_wait(smem_u32(fin), 0u, nullptr)) fail();
+      if (!mbar_wait(smem_u32(fin), 0u, nullptr, FIN_WAIT_LIMIT)) fail();
     }
     __syncwarp();
   } else {
@@ -447,12 +417,16 @@ grouped_zgemm_split_kernel(const GJob* __restrict__ jobs, int njobs, const GGrou
       double2* C = partial ? bases.part + job.part_off : bases.p[g.c_base] + g.c_off;
       const long long ldc = partial ? g.M : g.c_ld;
       const bool acc_old = !partial && g.beta;
+      const bool slice_out = !partial && g.s_off >= 0;
+      const int s_nks = (g.N + SP_TK - 1) / SP_TK;
+      const int npass = nseg > 0 ? nseg : 1;
       // one pass per accumulator segment (one pass of zeros for a job of element terms only);
       // the first writes beta * C_old + element terms + segment, later ones add to what it wrote
-      for (int sgi = 0; sgi < (nseg > 0 ? nseg : 1); ++sgi) {
+      for (int sgi = 0; sgi < npass; ++sgi) {
         const int a = sg & 1, ua = sg >> 1;
         if (nseg > 0) {
-          if (!mbar_wait(smem_u32(&accf[a]), (uint32_t)(ua & 1), abort_flag)) {
+          // warp-uniform: the tensor-memory loads below need every lane
+          if (!__all_sync(0xffffffffu, mbar_wait(smem_u32(&accf[a]), (uint32_t)(ua & 1), abort_flag, wait_limit))) {
             fail();
             ok = false;
             break;
@@ -533,6 +507,19 @@ grouped_zgemm_split_kernel(const GJob* __restrict__ jobs, int njobs, const GGrou
               const int col = n0 + c0 + j;
               if (col < g.N) C[(long long)row + (long long)col * ldc] = make_double2(cr[j], ci[j]);
             }
+            // a phase-1 intermediate read by the next launch as an A operand: its final
+            // values also go, sliced, into the A tiles of its view (rows >= M and columns
+            // >= N of those tiles stay zero from the arena's initial clearing)
+            if (slice_out && sgi == npass - 1) {
+              double2 v[8];
+#pragma unroll
+              for (int j = 0; j < 8; ++j)
+                v[j] = (n0 + c0 + j) < g.N ? make_double2(cr[j], ci[j]) : make_double2(0.0, 0.0);
+              const int col0 = n0 + c0;
+              const long long unit = g.s_off + 2ll * ((long long)job.tm * s_nks + col0 / SP_TK);
+              if (unit + 2 <= arenas.units[ARENA_T])
+                store_chunk(arenas.a[ARENA_T] + unit * SPLIT_UNIT, A_PLANE, chunk_off(row - m0, (col0 / 8) & 1), v);
+            }
           }
         }
         if (nseg > 0) sg++;
@@ -550,8 +537,10 @@ grouped_zgemm_split_kernel(const GJob* __restrict__ jobs, int njobs, const GGrou
 }  // namespace
 
 cudaError_t launch_grouped_zgemm_split(const GJob* jobs, int njobs, const GGroup* groups, const GTerm* terms,
-                                       Bases bases, cudaStream_t st) {
+                                       Bases bases, SplitArenas arenas, int* fault, long long wait_limit,
+                                       cudaStream_t st) {
   if (njobs <= 0) return cudaSuccess;
+  if (!fault || wait_limit < 0) return cudaErrorInvalidValue;
   static std::atomic<unsigned long long> attr{0};
   cudaError_t e = ensure_smem_attr(grouped_zgemm_split_kernel, SMEM_BYTES, attr);
   if (e != cudaSuccess) return e;
@@ -560,15 +549,16 @@ cudaError_t launch_grouped_zgemm_split(const GJob* jobs, int njobs, const GGroup
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
   if (nsm <= 0) nsm = 148;
   const int grid = njobs < nsm ? njobs : nsm;
-  grouped_zgemm_split_kernel<<<grid, SP_THREADS, SMEM_BYTES, st>>>(jobs, njobs, groups, terms, bases);
+  grouped_zgemm_split_kernel<<<grid, SP_THREADS, SMEM_BYTES, st>>>(jobs, njobs, groups, terms, bases, arenas,
+                                                                    fault, wait_limit);
   return cudaGetLastError();
 }
 
-cudaError_t split_fault_flag(int* host_flag, int clear) {
-  cudaError_t e = cudaMemcpyFromSymbol(host_flag, g_split_fault, sizeof(int));
-  if (e != cudaSuccess || !clear) return e;
-  const int zero = 0;
-  return cudaMemcpyToSymbol(g_split_fault, &zero, sizeof(int));
+cudaError_t launch_slice_tiles(const SView* views, const STile* tiles, int ntiles, const double2* in,
+                               unsigned char* arena, long long arena_units, cudaStream_t st) {
+  if (ntiles <= 0) return cudaSuccess;
+  slice_tiles_kernel<<<ntiles, 256, 0, st>>>(views, tiles, in, arena, arena_units);
+  return cudaGetLastError();
 }
 
 }  // namespace tsc

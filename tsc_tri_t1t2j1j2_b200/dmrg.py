@@ -111,6 +111,32 @@ class Context:
         superblock set."""
         self._check(self.L.tsc_set_precision(self.h, int(mode), float(split_tol)))
 
+    def set_split_wait_limit(self, polls: int):
+        """Poll limit of the split kernel's bounded waits (default 1<<20; 0 makes
+        every wait give up at once, so the next split call fails with TSC_E_CUDA)."""
+        self._check(self.L.tsc_set_split_wait_limit(self.h, int(polls)))
+
+    def split_views(self):
+        """Bytes and counts of the split form's pre-sliced operand views of the current
+        superblock: {"operators": (bytes, views), "input": ..., "intermediates": ...}."""
+        b, v = (ctypes.c_longlong * 3)(), (ctypes.c_int * 3)()
+        self._check(self.L.tsc_split_views(self.h, b, v))
+        return {k: (b[i], v[i]) for i, k in enumerate(("operators", "input", "intermediates"))}
+
+    def set_resident_limit(self, nbytes: int):
+        """Device bytes the stored block models may hold before the least recently
+        used move to host memory (< 0: 45 % of the device, the default; 0: all)."""
+        self._check(self.L.tsc_set_resident_limit(self.h, int(nbytes)))
+
+    def spill_stats(self):
+        """{spills, restores, bytes, seconds, resident_bytes, limit_bytes} of the stored models."""
+        sp, rs, rb, lb = ctypes.c_longlong(), ctypes.c_longlong(), ctypes.c_longlong(), ctypes.c_longlong()
+        by, sec = ctypes.c_double(), ctypes.c_double()
+        self._check(self.L.tsc_spill_stats(self.h, ctypes.byref(sp), ctypes.byref(rs), ctypes.byref(by),
+                                           ctypes.byref(sec), ctypes.byref(rb), ctypes.byref(lb)))
+        return {"spills": sp.value, "restores": rs.value, "bytes": by.value, "seconds": sec.value,
+                "resident_bytes": rb.value, "limit_bytes": lb.value}
+
     def blocksparse_set(self, problems):
         """Block-sparse batch (tsc_blocksparse_set): `problems` is a list of
         blocksparse.Problem; returns (psi length, algorithmic flops of one
