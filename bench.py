@@ -1,20 +1,27 @@
 #!/usr/bin/env python
 """Benchmark of the superblock hot path: H.psi (model_wave, get_sys.f90:6915) on
-the YC4x12 (config 2: 48 sites, 44 electrons, t1=1, t2=0.3, J1=0.4, J2=0.036)
-superblock sys=23 | 2 sites | env=23 at m=1000 kept SU(2) multiplets.
+the YC4x24 superblock of the benchmark list's config 3 (96 sites, 88
+electrons, t1=1, t2=0.3, J1=0.4, J2=0.036) at the middle of the lattice,
+sys=47 | 2 sites | env=47, keeping m=4000 SU(2) multiplets.
 
-The sector structure is the one the engine's own warm-up produces
-(tests/golden/superblock_yc4x12_m1000.npz, made by make_bench_superblock.py);
-operator and psi values are seeded random (complex N(0,1), Hermitian diagonal
-blocks), identical for every arm.  A step is one H.psi application.
+The sector structure is the one the engine's own warm-up to m=4000 produces
+(tests/golden/superblock_yc4x24_m4000.npz, made by
+tests/golden/make_bench_superblock.py); operator and psi values are seeded
+random (complex N(0,1), Hermitian diagonal blocks), identical for every arm.  A
+step is one H.psi application.  `--config 2` puts the YC4x12 m=1000 superblock
+(config 2) in the headline instead; it is always measured as a side leg.
 
-  python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+  python bench.py [--gpus N --steps K --warmup W] [--impl reference] [--config 2|3]
 
 Prints one JSON line (rank 0).  value = algorithmic TFLOP/s (flops counted in
-the reference's GEMM association order, 8*m*n*k per complex GEMM) of all ranks;
-N>1 runs independent replicas (the path does not shard).  Rank 0 adds the
-split-precision form on the same superblock ("split") and the whole YC4x12
-ground-state search in both forms ("sweep": seconds per sweep, energies).
+the reference's GEMM association order, 8*m*n*k per complex GEMM) of all ranks
+in the plain FP64 form; N>1 runs independent replicas (the path does not
+shard).  Rank 0 adds the split-precision form on the same superblock
+("split", with its speed-up over FP64 and its error), the config-2 superblock
+in both forms ("config2_hpsi"), the whole YC4x12 ground-state search in both
+forms with per-phase seconds ("sweep"), the reference's CPU-runnable case
+whole beside the CPU oracle ("sweep_config1"), parameter points and the
+synthetic block-sparse H.psi ("config5").
 """
 from __future__ import annotations
 
@@ -32,11 +39,16 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 FIXTURE = os.path.join(ROOT, "tests", "golden", "superblock_yc4x12_m1000.npz")
 MODEL = dict(Nx=12, Ny=4, t1=1.0, t2=0.3, J1=0.4, J2=0.036, delta=12)
+FIXTURE3 = os.path.join(ROOT, "tests", "golden", "superblock_yc4x24_m4000.npz")
+MODEL3 = dict(Nx=24, Ny=4, t1=1.0, t2=0.3, J1=0.4, J2=0.036, delta=12)
 SEED = 20240601
 BASELINE_METRIC = "sweep sec & H·psi TFLOP/s: split-prec batched vs FP64 GPU at |dE/E|<=1e-10"
 METRIC = "H·psi TFLOP/s (plain complex-FP64 GPU form, algorithmic flops)"
 WORKLOAD = ("YC4x12 (48 sites, 44 e-, S=0, t1=1 t2=0.3 J1=0.4 J2=0.036) superblock sys=23|2|env=23 "
             "at m=1000 multiplets; one H.psi (model_wave) per step")
+WORKLOAD3 = ("YC4x24 (96 sites, 88 e-, S=0, t1=1 t2=0.3 J1=0.4 J2=0.036) superblock sys=47|2|env=47 "
+             "at m=4000 multiplets (structure of the engine's warm-up to m=4000); one H.psi (model_wave) per step")
+HEADLINES = {2: (FIXTURE, MODEL, WORKLOAD), 3: (FIXTURE3, MODEL3, WORKLOAD3)}
 
 
 # ----------------------------------------------------------------------------- workload
@@ -98,9 +110,9 @@ def scale_dims(ints, k):
     return x.astype(np.int32)
 
 
-def make_superblock(seed=SEED, scale=1):
+def make_superblock(seed=SEED, scale=1, fixture=FIXTURE):
     """Fixture descriptors + seeded values -> (sys_len, env_len, ints, data, psi_offset, n)."""
-    z = np.load(FIXTURE)
+    z = np.load(fixture)
     ints = scale_dims(z["ints"].astype(np.int32), scale)
     rng = np.random.default_rng(seed)
     chunks = []
@@ -235,13 +247,13 @@ def fp64_peak_tflops(torch, dev):
     return best
 
 
-def cpu_hpsi(sb, nreps):
+def cpu_hpsi(sb, nreps, model=MODEL):
     """Oracle (CPU restatement of the reference) H.psi on the same superblock."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import orc
     sl, el, ints, data, _off, n = sb
-    o = orc.Oracle(orc.RunConfig(Nx=MODEL["Nx"], Ny=MODEL["Ny"], t1=MODEL["t1"], t2=MODEL["t2"],
-                                 J1=MODEL["J1"], J2=MODEL["J2"], delta=MODEL["delta"], sweeps=[1]))
+    o = orc.Oracle(orc.RunConfig(Nx=model["Nx"], Ny=model["Ny"], t1=model["t1"], t2=model["t2"],
+                                 J1=model["J1"], J2=model["J2"], delta=model["delta"], sweeps=[1]))
     t0 = time.perf_counter()
     out, sec, flops = o.hpsi_flat(sl, el, ints, data, n, nreps=nreps)
     wall = time.perf_counter() - t0
@@ -253,12 +265,16 @@ def run_reference(args):
     dist, rank, ws, _local = dist_setup()
     if rank != 0:
         return 0
-    sb = make_superblock()
+    fixture, model, workload = HEADLINES[args.config]
+    sb = make_superblock(fixture=fixture)
     # bounded sample: at most ~60 s of CPU work whatever K is
-    out, sec1, flops, _ = cpu_hpsi(sb, 1)
+    out, sec1, flops, _ = cpu_hpsi(sb, 1, model)
     per = max(sec1, 1e-6)
     k = max(1, min(args.steps, int(60.0 / per)))
-    _, sec, flops, wall = cpu_hpsi(sb, k)
+    if k > 1:
+        _, sec, flops, wall = cpu_hpsi(sb, k, model)
+    else:
+        sec = sec1
     value = flops / sec / 1e12
     cores = os.cpu_count()
     line = {
@@ -266,7 +282,7 @@ def run_reference(args):
         "unit": "TFLOP/s", "n_gpus": args.gpus, "steps": k, "warmup": 1, "ms_per_step": sec * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128",
         "data": "synthetic: engine-recorded sector structure, seeded N(0,1) values",
-        "config": {"workload": WORKLOAD, "parallelism": "cpu threads (OpenBLAS)", "cache": "inputs > L2"},
+        "config": {"workload": workload, "parallelism": "cpu threads (OpenBLAS)", "cache": "inputs > L2"},
         "cpu_baseline": {"value": value, "unit": "TFLOP/s", "cores": cores, "kind": "port",
                          "sample": f"{k} of {args.steps} H.psi steps (bounded to ~60 s), OpenBLAS threads={cores}; "
                                    "the reference Fortran cannot be compiled here (no Fortran compiler)"},
@@ -285,11 +301,11 @@ def measured_bf16_peak():
         return 1590.0, "fallback 1.59 PFLOP/s"
 
 
-def split_leg(torch, dev, sb, steps, fp64_out):
+def split_leg(torch, dev, sb, steps, fp64_out, model=MODEL, fp64_ms=None):
     """The split-precision form (BF16 slices on tcgen05) on the same superblock and psi."""
     from tsc_tri_t1t2j1j2_b200 import Context
     sl, el, ints, data, off, n = sb
-    ctx = Context(device=dev.index, **MODEL)
+    ctx = Context(device=dev.index, **model)
     ctx.set_precision(Context.SPLIT_BF16)
     ctx.set_superblock_flat(sl, el, ints, data)
     stream = torch.cuda.ExternalStream(ctx.stream, device=dev)
@@ -307,6 +323,7 @@ def split_leg(torch, dev, sb, steps, fp64_out):
         ms += ctx.hpsi_stats()["device_ms"]
     ms /= steps
     st = ctx.hpsi_stats()
+    views = ctx.split_views()
     ctx.close()
     got = out.cpu().numpy()
     err = float(np.max(np.abs(got - fp64_out)) / np.max(np.abs(fp64_out)))
@@ -316,7 +333,9 @@ def split_leg(torch, dev, sb, steps, fp64_out):
     peak, src = measured_bf16_peak()
     achieved = bf16_flops / (ms * 1e-3) / 1e12
     return {"hpsi_tflops": st["ref_flops"] / (ms * 1e-3) / 1e12, "ms_per_hpsi": ms,
+            "hpsi_speedup_over_fp64": (fp64_ms / ms) if fp64_ms else None,
             "max_rel_err_vs_fp64": err, "tolerance": 2e-5,
+            "sliced_operand_bytes": {k: v[0] for k, v in views.items()},
             "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                          "frac": achieved / peak, "peak_source": src,
                          "note": "BF16 tensor flops executed (6x the task list's complex flops)",
@@ -497,20 +516,14 @@ def points_leg(dev):
             "final_e0_max_rel_diff": max(abs(a - b) / abs(b) for a, b in zip(par, seq))}
 
 
-def run_gpu(args):
-    import torch
+def fp64_hpsi(torch, dev, sb, model, steps, warmup, dist=None, clocks=None):
+    """The plain FP64 form on one superblock: the autotuner's schedule, `steps`
+    H.psi timed back to back by CUDA events on the engine stream (one barrier and
+    synchronisation on each side), and the mean device time of one H.psi's
+    grouped-GEMM launches.  Returns (ctx, psi, out, result dict)."""
     from tsc_tri_t1t2j1j2_b200 import Context
-    from tsc_tri_t1t2j1j2_b200 import _lib
-    dist, rank, ws, local = dist_setup()
-    if dist is not None:
-        import datetime
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
-    dev = torch.device("cuda", local)
-    torch.cuda.set_device(dev)
-    sb = make_superblock(scale=args.scale)
     sl, el, ints, data, off, n = sb
-    ctx = Context(device=local, **MODEL)
+    ctx = Context(device=dev.index, **model)
     ctx.set_superblock_flat(sl, el, ints, data)
     assert ctx.dim == n
     stream = torch.cuda.ExternalStream(ctx.stream, device=dev)
@@ -519,33 +532,55 @@ def run_gpu(args):
     psi = torch.from_numpy(data[off:off + n].copy()).to(dev)
     out = torch.empty_like(psi)
     torch.cuda.synchronize()
-    for _ in range(args.warmup):
+    for _ in range(warmup):
         ctx.hpsi_device(psi.data_ptr(), out.data_ptr())
     torch.cuda.synchronize()
-    ref_flops = ctx.hpsi_stats()["ref_flops"]
-    exec_flops = ctx.hpsi_stats()["exec_flops"]
+    st = ctx.hpsi_stats()
     if dist is not None:
         dist.barrier()
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with ClockSampler(local) as clocks:
-        e0.record(stream)
-        for _ in range(args.steps):
-            ctx.hpsi_device(psi.data_ptr(), out.data_ptr())
-        e1.record(stream)
-        e1.synchronize()
+    sampler = ClockSampler(dev.index) if clocks else None
+    if sampler:
+        sampler.__enter__()
+    e0.record(stream)
+    for _ in range(steps):
+        ctx.hpsi_device(psi.data_ptr(), out.data_ptr())
+    e1.record(stream)
+    e1.synchronize()
+    if sampler:
+        sampler.__exit__()
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1)
     if dist is not None:
         ms = max_over_ranks(ms, dist, dev)
         dist.barrier()
-    value = ws * args.steps * ref_flops / (ms * 1e-3) / 1e12
-    # per-launch kernel time of the grouped GEMM (both H.psi launches), CUDA events on the engine stream
     kms = []
-    for _ in range(20):
+    for _ in range(min(20, max(3, steps))):
         ctx.hpsi_device(psi.data_ptr(), out.data_ptr())
         kms.append(ctx.hpsi_stats()["device_ms"])
-    kernel_ms = float(np.mean(kms))
+    res = {"ms_total": ms, "ms_per_step": ms / steps, "ref_flops": st["ref_flops"], "exec_flops": st["exec_flops"],
+           "kernel_ms": float(np.mean(kms)), "schedule": schedule, "tune_table": tune_table,
+           "clocks": sampler.summary() if sampler else None, "psi_amplitudes": n, "operator_elements": int(off)}
+    return ctx, psi, out, res
+
+
+def run_gpu(args):
+    import torch
+    from tsc_tri_t1t2j1j2_b200 import _lib
+    dist, rank, ws, local = dist_setup()
+    if dist is not None:
+        import datetime
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    fixture, model, workload = HEADLINES[args.config]
+    sb = make_superblock(scale=args.scale, fixture=fixture)
+    sl, el, ints, data, off, n = sb
+    ctx, psi, out, r = fp64_hpsi(torch, dev, sb, model, args.steps, args.warmup, dist, clocks=True)
+    ms, ref_flops, exec_flops, kernel_ms = r["ms_total"], r["ref_flops"], r["exec_flops"], r["kernel_ms"]
+    value = ws * args.steps * ref_flops / (ms * 1e-3) / 1e12
     # end to end through the C-ABI: pinned host psi -> device -> H.psi -> host
     xh = torch.from_numpy(data[off:off + n].copy()).pin_memory()
     yh = torch.empty_like(xh).pin_memory()
@@ -565,6 +600,9 @@ def run_gpu(args):
     if dist is not None:
         e2e_s = max_over_ranks(e2e_s, dist, dev)
     e2e = ws * ke2e * ref_flops / e2e_s / 1e12
+    gpu_out = out.cpu().numpy()
+    ctx.close()
+    del psi, out
     line = None
     if rank == 0:
         peak = fp64_peak_tflops(torch, dev)
@@ -573,25 +611,29 @@ def run_gpu(args):
             "metric": METRIC, "baseline_metric": BASELINE_METRIC, "value": value, "unit": "TFLOP/s",
             "n_gpus": ws, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128",
-            "data": "synthetic: engine-recorded sector structure (tests/golden/superblock_yc4x12_m1000.npz), "
+            "data": f"synthetic: engine-recorded sector structure ({os.path.relpath(fixture, ROOT)}), "
                     "seeded N(0,1) complex values",
-            "config": {"workload": WORKLOAD if args.scale == 1 else
-                       WORKLOAD + f"; every dimension scaled x{args.scale} (synthetic m ~ {1000 * args.scale} size class)",
+            "config": {"workload": workload if args.scale == 1 else
+                       workload + f"; every dimension scaled x{args.scale}",
                        "psi_amplitudes": n, "operator_elements": int(off),
                        "ref_gflop_per_step": ref_flops / 1e9, "exec_gflop_per_step": exec_flops / 1e9,
                        "parallelism": f"replicas x{ws}", "cache": f"inputs > L2 (operators {16 * off / 1e6:.0f} MB)"},
             "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                         "frac": achieved / peak, "traffic": TRAFFIC_BYTES_PER_STEP if args.scale == 1 else None,
+                         "frac": achieved / peak, "traffic": None,
+                         "algorithmic_bytes": traffic_model(sb),
+                         "algorithmic_bytes_note": "every operator sub-block and psi element read once, every "
+                                                   "output element written once, per H.psi",
                          "peak_source": "cuBLAS ZGEMM 4096^3 complex128 measured in this run (FP64 DMMA)",
                          "kernel": "grouped_zgemm (2 launches per H.psi)",
-                         "schedule": {"tile": schedule[0], "waves": schedule[1],
-                                      "candidates_ms_per_gflop": {str(k): v for k, v in tune_table.items()}}},
+                         "schedule": {"tile": r["schedule"][0], "waves": r["schedule"][1],
+                                      "candidates_ms_per_gflop": {str(k): v for k, v in r["tune_table"].items()}}},
             "e2e": {"value": e2e, "unit": "TFLOP/s", "h2d_bytes_per_step": 16 * n, "d2h_bytes_per_step": 16 * n},
             "gpu_launches": 2 * args.steps,
-            "clocks": clocks.summary(),
+            "clocks": r["clocks"],
         }
-        gpu_out = out.cpu().numpy()
-        line["split"] = split_leg(torch, dev, sb, max(20, args.steps // 4), gpu_out)
+        line["split"] = split_leg(torch, dev, sb, max(10, args.steps // 4), gpu_out, model, r["kernel_ms"])
+        if args.config != 2:
+            line["config2_hpsi"] = config2_leg(torch, dev, args.warmup)
         if not args.no_synthetic:
             line["config5"] = config5_leg(torch, dev, peak)
         if not args.no_sweep:
@@ -599,13 +641,12 @@ def run_gpu(args):
             line["sweep_config1"] = config1_leg(dev, ws == 1 and not args.no_cpu)
             line["parameter_points"] = points_leg(dev)
         if ws == 1 and not args.no_cpu:
-            cpu_out, sec, flops, wall = cpu_hpsi(sb, 1)
+            cpu_out, sec, flops, wall = cpu_hpsi(sb, 1, model)
             err = float(np.max(np.abs(gpu_out - cpu_out)) / np.max(np.abs(cpu_out)))
             line["cpu_baseline"] = {"value": flops / sec / 1e12, "unit": "TFLOP/s", "cores": os.cpu_count(),
                                     "kind": "port", "sample": "1 H.psi of the same superblock (oracle, OpenBLAS "
                                                               f"threads={os.cpu_count()}), {sec:.2f} s"}
             line["parity"] = {"max_rel_err_vs_oracle": err, "tolerance": 1e-13}
-    ctx.close()
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
@@ -614,22 +655,37 @@ def run_gpu(args):
     return 0
 
 
-# bytes the dominant kernel moves per H.psi (dram__bytes_read.sum + dram__bytes_write.sum
-# of its two launches), from one ncu capture of this workload
-# (profiles/hpsi_grouped_zgemm_yc4x12_m1000.md): phase 1 0.0917 + 0.3857 GB,
-# phase 2 1.3513 + 0.0816 GB
-TRAFFIC_BYTES_PER_STEP = 1.9103e9
+def config2_leg(torch, dev, warmup):
+    """The config-2 superblock (YC4x12 m=1000) in both forms: FP64 TFLOP/s, split
+    TFLOP/s, the split/FP64 time ratio and the split form's error."""
+    sb = make_superblock()
+    ctx, psi, out, r = fp64_hpsi(torch, dev, sb, MODEL, 20, warmup)
+    fp64_out = out.cpu().numpy()
+    ctx.close()
+    res = {"workload": WORKLOAD, "fp64": {"ms_per_hpsi": r["ms_per_step"], "kernel_ms": r["kernel_ms"],
+                                          "hpsi_tflops": r["ref_flops"] / (r["ms_per_step"] * 1e-3) / 1e12}}
+    res["split"] = split_leg(torch, dev, sb, 20, fp64_out, MODEL, r["kernel_ms"])
+    return res
+
+
+def traffic_model(sb):
+    """Bytes one H.psi must move at least: the superblock's operator sub-blocks and
+    psi read once (16 B per complex element) and the output written once."""
+    _sl, _el, _ints, _data, off, n = sb
+    return 16 * (int(off) + 2 * int(n))
 
 
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=400)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-sweep", action="store_true", help="skip the whole-run (sweep seconds) leg")
     ap.add_argument("--no-synthetic", action="store_true", help="skip the synthetic block-sparse leg")
+    ap.add_argument("--config", type=int, default=3 if os.path.exists(FIXTURE3) else 2, choices=[2, 3],
+                    help="headline superblock: 3 = YC4x24 m=4000 (default), 2 = YC4x12 m=1000")
     ap.add_argument("--scale", type=int, default=1,
                     help="multiply every dimension of the superblock by this (4: m ~ 4000 size class)")
     args = ap.parse_args()

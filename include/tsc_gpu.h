@@ -56,6 +56,9 @@ typedef struct tsc_sweep_config {
   int warmup_only;         /* 1: stop after warm_up_point (dmrg_sub.f90:974-1147) */
   int final_half_sweep;    /* 1: end with left_to_right up to 5*Num_site/6 (main.f90:205-206),
                             * the position where the reference measures */
+  int resume;              /* 1: skip the warm-up and the two half sweeps and run the sweeps
+                            * from the state tsc_checkpoint_read loaded (the reference's
+                            * restart1 = 1 from restart.dat, main.f90:36-38, 147-174) */
 } tsc_sweep_config;
 
 /* One record per Lanczos solve (eigen.f90:169-173, den_mat.f90:342-350). */
@@ -181,6 +184,21 @@ int tsc_measure_density(tsc_ctx* ctx, double* out, int nsites);
  * Nx*Ny values, out[j-1] = Re <n_site n_j> for those j and 0 elsewhere (as the
  * reference's zero-initialised correlation matrix row); returns Nx*Ny. */
 int tsc_measure_density_cor(tsc_ctx* ctx, int site, double* out, int nsites);
+
+/* Checkpoint in the reference's file format (names dmrg_sub.f90:657-709):
+ * writes into directory dir, for every model, truncation and basis the last
+ * tsc_dmrg_run stored, the files sysblocks<i> / envblocks<i> (model_to_disk,
+ * block.f90:1802-1845), systruns<i> / envtruns<i> (truns_to_disk, :1936-1956),
+ * sysbs<i> / envbs<i> (basis_to_disk, :1983-2026, formatted) and eigvec1, the
+ * last wavefunction (wave_to_disk, :1547-1576).  Unformatted files are Fortran
+ * sequential records with 4-byte length markers, 4-byte integers and 16-byte
+ * complex values, as gfortran and ifort write them.  Returns the number of
+ * files written.  A run that ended with a full sweep leaves the wave at the
+ * left end, where a resumed run starts. */
+int tsc_checkpoint_write(tsc_ctx* ctx, const char* dir);
+/* Reads such a file set (all lengths 1..Nx*Ny present in dir) into the
+ * context; tsc_dmrg_run with resume = 1 then continues from it. */
+int tsc_checkpoint_read(tsc_ctx* ctx, const char* dir);
 
 /* Serialises the superblock of the most recent step of tsc_dmrg_run whose
  * global solve index equals capture_step (set before the run with

@@ -21,6 +21,7 @@ EXPORTED = [
     "tsc_renormalize", "tsc_wave_transform", "tsc_dmrg_run", "tsc_set_capture", "tsc_get_capture",
     "tsc_hpsi_stats", "tsc_stream", "tsc_hpsi_noalloc", "tsc_set_precision", "tsc_set_split_wait_limit",
     "tsc_set_resident_limit", "tsc_spill_stats", "tsc_split_views",
+    "tsc_checkpoint_write", "tsc_checkpoint_read",
     "tsc_blocksparse_set", "tsc_blocksparse_apply", "tsc_measure_density", "tsc_measure_density_cor", "tsc_set_autotune",
     "tsc_autotune_table", "tsc_autotune_superblock",
 ]
@@ -34,7 +35,7 @@ class ModelConfig(ctypes.Structure):
 class SweepConfig(ctypes.Structure):
     _fields_ = [("kept_min", c_int), ("kept_max_warmup", c_int), ("nsweeps", c_int),
                 ("sweep_kept_max", P(c_int)), ("lanzero", c_double), ("seed", ctypes.c_ulonglong),
-                ("warmup_only", c_int), ("final_half_sweep", c_int)]
+                ("warmup_only", c_int), ("final_half_sweep", c_int), ("resume", c_int)]
 
 
 class StepLog(ctypes.Structure):
@@ -91,6 +92,8 @@ def load():
     L.tsc_set_split_wait_limit.argtypes = [c_void, c_ll]
     L.tsc_set_resident_limit.argtypes = [c_void, c_ll]
     L.tsc_split_views.argtypes = [c_void, P(c_ll), P(c_int)]
+    L.tsc_checkpoint_write.argtypes = [c_void, ctypes.c_char_p]
+    L.tsc_checkpoint_read.argtypes = [c_void, ctypes.c_char_p]
     L.tsc_spill_stats.argtypes = [c_void, P(c_ll), P(c_ll), P(c_double), P(c_double), P(c_ll), P(c_ll)]
     L.tsc_blocksparse_set.argtypes = [c_void, c_int, ctypes.POINTER(c_int), c_ll, ctypes.POINTER(c_double), c_ll,
                                       ctypes.POINTER(c_ll), ctypes.POINTER(c_double), ctypes.POINTER(c_double)]

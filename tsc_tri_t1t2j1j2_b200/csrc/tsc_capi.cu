@@ -334,7 +334,7 @@ int tsc_dmrg_run(tsc_ctx* ctx, const tsc_sweep_config* sw, tsc_step_log* log, in
     std::vector<int> sweeps(sw->sweep_kept_max, sw->sweep_kept_max + sw->nsweeps);
     std::vector<Engine::StepRec> recs;
     ctx->eng->run(sw->kept_min, sw->kept_max_warmup, sweeps, sw->lanzero, sw->seed, &recs, sw->warmup_only != 0,
-                  sw->final_half_sweep != 0);
+                  sw->final_half_sweep != 0, sw->resume != 0);
     nsteps = (int)recs.size();
     for (int i = 0; i < nsteps && i < max_steps && log; ++i) {
       const auto& s = recs[i];

@@ -1459,29 +1459,36 @@ void Engine::right_to_left(int bg_id, int end_id, double trun_err, std::vector<S
 }
 
 void Engine::run(int kept_min, int kept_warm, const std::vector<int>& sweeps, double lanzero_override,
-                 unsigned long long seed, std::vector<StepRec>* log, bool warmup_only, bool final_half) {
+                 unsigned long long seed, std::vector<StepRec>* log, bool warmup_only, bool final_half, bool resume) {
   const int N = L.num_site;
   rng = seed;
   nsolve_ = 0;
-  models_.clear();
   models_.bind(st);
-  sys_truns.clear();
-  env_truns.clear();
-  sys_bsm.clear();
-  env_bsm.clear();
   const double lanerr = (double)1.0e-6f, trun_err = 1.0000000036274937e-15;
   auto lz = [&](double v) { return lanzero_override > 0 ? lanzero_override : v; };
   kept_min_ = kept_min;
   kept_max_ = kept_warm;
-  restart1 = 0;
-  lanzero_ = lz(lanerr * 1000);
-  warm_up(N / 2, trun_err * 100, log);
-  if (warmup_only) return;
-  lanzero_ = lz(lanerr * 15);
   double tmp_err = trun_err * 15;
-  left_to_right(N / 2 - 1, N - 2, tmp_err, log);
-  restart1 = 1;
-  right_to_left(N - 2, 1, tmp_err, log);
+  if (resume) {
+    // the stores hold the checkpoint's models, truncations, bases and wave
+    if (!resume_ready_) throw Error(-4, "resume: no checkpoint has been read");
+    restart1 = 1;
+  } else {
+    models_.clear();
+    sys_truns.clear();
+    env_truns.clear();
+    sys_bsm.clear();
+    env_bsm.clear();
+    restart1 = 0;
+    lanzero_ = lz(lanerr * 1000);
+    warm_up(N / 2, trun_err * 100, log);
+    if (warmup_only) return;
+    lanzero_ = lz(lanerr * 15);
+    left_to_right(N / 2 - 1, N - 2, tmp_err, log);
+    restart1 = 1;
+    right_to_left(N - 2, 1, tmp_err, log);
+  }
+  resume_ready_ = false;
   for (size_t it = 1; it <= sweeps.size(); ++it) {
     kept_max_ = sweeps[it - 1];
     if (kept_min_ > kept_max_) kept_min_ = kept_max_;

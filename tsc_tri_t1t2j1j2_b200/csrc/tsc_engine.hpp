@@ -182,6 +182,11 @@ class ModelStore {
   void put(int side, int len, const DModel& m);   // store; may spill older models
   DModel get(int side, int len);                  // resident copy (restored if spilled)
   bool has(int side, int len) const { return map_.count(key(side, len)) > 0; }
+  std::vector<std::pair<int, int>> keys() const {   // (side, length) of every stored model
+    std::vector<std::pair<int, int>> k;
+    for (const auto& kv : map_) k.push_back({(int)(kv.first >> 32), (int)(kv.first & 0xffffffff)});
+    return k;
+  }
   void clear() { map_.clear(); resident_ = 0; }
   void bind(cudaStream_t st) { st_ = st; }
   // bytes of device memory the stored models may hold; < 0: 45 % of the device
@@ -382,8 +387,15 @@ class Engine {
     int split_iters;
     double split_e0;
   };
+  // resume: skip the warm-up and the two half sweeps and continue with the
+  // sweeps from the state checkpoint_read loaded (restart1 = 1, main.f90:36-38)
   void run(int kept_min, int kept_warm, const std::vector<int>& sweeps, double lanzero_override,
-           unsigned long long seed, std::vector<StepRec>* log, bool warmup_only = false, bool final_half = false);
+           unsigned long long seed, std::vector<StepRec>* log, bool warmup_only = false, bool final_half = false,
+           bool resume = false);
+  // the reference's checkpoint files (tsc_checkpoint.cu): every stored model,
+  // truncation and basis of the last run and its last wavefunction
+  int checkpoint_write(const std::string& dir);
+  void checkpoint_read(const std::string& dir);
   int capture_step = -1;
   struct Capture {
     bool valid = false;
@@ -426,6 +438,7 @@ class Engine {
   WLayout disk_layout;
   DevBufP disk_wave;
   int restart1 = 0;
+  bool resume_ready_ = false;   // checkpoint_read has loaded a state to continue from
   int kept_min_ = 0, kept_max_ = 0;
   double lanzero_ = 0;
   int nsolve_ = 0;

@@ -509,8 +509,10 @@ grouped_zgemm_split_kernel(const GJob* __restrict__ jobs, int njobs, const GGrou
             }
             // a phase-1 intermediate read by the next launch as an A operand: its final
             // values also go, sliced, into the A tiles of its view (rows >= M and columns
-            // >= N of those tiles stay zero from the arena's initial clearing)
-            if (slice_out && sgi == npass - 1) {
+            // >= N of those tiles stay zero from the arena's initial clearing).  Column
+            // chunks past the view's last k-step belong to no tile of this row: writing
+            // them would land in the next row tile's tiles.
+            if (slice_out && sgi == npass - 1 && (n0 + c0) / SP_TK < s_nks) {
               double2 v[8];
 #pragma unroll
               for (int j = 0; j < 8; ++j)

@@ -20,6 +20,7 @@ status code and message on failure.
 from __future__ import annotations
 
 import ctypes
+import os
 
 import numpy as np
 
@@ -122,6 +123,16 @@ class Context:
         b, v = (ctypes.c_longlong * 3)(), (ctypes.c_int * 3)()
         self._check(self.L.tsc_split_views(self.h, b, v))
         return {k: (b[i], v[i]) for i, k in enumerate(("operators", "input", "intermediates"))}
+
+    def checkpoint_write(self, directory) -> int:
+        """Writes the last run's stored models, truncations, bases and wave as the
+        reference's checkpoint files (sysblocks<i>, systruns<i>, sysbs<i>, env...,
+        eigvec1) into `directory`; returns the number of files."""
+        return self._check(self.L.tsc_checkpoint_write(self.h, os.fsencode(directory)))
+
+    def checkpoint_read(self, directory):
+        """Loads such a file set; get_ground_state(..., resume=True) continues from it."""
+        self._check(self.L.tsc_checkpoint_read(self.h, os.fsencode(directory)))
 
     def set_resident_limit(self, nbytes: int):
         """Device bytes the stored block models may hold before the least recently
@@ -243,11 +254,13 @@ class Context:
 
     # ------------------------------------------------------------------ full run
     def get_ground_state(self, kept_min, kept_warm, sweeps, lanzero=-1.0, seed=1, capture_step=-1, max_steps=100000,
-                         warmup_only=False, final_half_sweep=False):
+                         warmup_only=False, final_half_sweep=False, resume=False):
+        """Get_Ground_State (main.f90:114-209); resume=True continues with the sweeps
+        from the state checkpoint_read loaded (no warm-up, no first half sweeps)."""
         self._check(self.L.tsc_set_capture(self.h, capture_step))
         sk = (ctypes.c_int * max(1, len(sweeps)))(*sweeps)
         cfg = _lib.SweepConfig(kept_min, kept_warm, len(sweeps), sk, lanzero, seed, 1 if warmup_only else 0,
-                               1 if final_half_sweep else 0)
+                               1 if final_half_sweep else 0, 1 if resume else 0)
         logs = (_lib.StepLog * max_steps)()
         n = self._check(self.L.tsc_dmrg_run(self.h, ctypes.byref(cfg), logs, max_steps))
         out = []
