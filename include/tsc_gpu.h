@@ -221,17 +221,27 @@ void* tsc_stream(tsc_ctx* ctx);
  * complex FP64 and has no such switch).  TSC_FP64: complex FP64 throughout.
  * TSC_SPLIT_BF16: every FP64 operand split into three BF16 slices multiplied
  * on the tensor cores with FP32 accumulators restarted every 128 of the inner
- * dimension and summed in FP64 (a few 1e-7 relative error per H.psi); Lanczos iterates on that H.psi until successive Ritz values agree to
- * split_tol relative (<= 0 keeps the current value, 1e-9 at creation), then
- * runs the reference's FP64 iterations from that vector until the FP64
- * residual ||H psi - E psi|| is below 0.1 sqrt(lanzero), so the energy and
- * vector it returns are FP64 results.  Orthogonalisation, tridiagonal solve,
+ * dimension and summed in FP64 (a few 1e-7 relative error per H.psi; the
+ * operator slices, with the terms' coefficients folded in, are built when the
+ * superblock is set); Lanczos iterates on that H.psi until successive Ritz
+ * values agree to split_tol relative (<= 0 keeps the current value, 1e-9 at
+ * creation), then runs the reference's FP64 iterations from that vector, with
+ * the reference's stop unless tsc_set_split_refinement asks for a residual
+ * bound, so the energy and vector it returns are FP64 results.  Orthogonalisation, tridiagonal solve,
  * density-matrix eigensolver, renormalisation and wave transforms stay FP64,
  * and so do the warm-up steps of tsc_dmrg_run.  Takes effect from the next
  * superblock set. */
 #define TSC_FP64 0
 #define TSC_SPLIT_BF16 1
 int tsc_set_precision(tsc_ctx* ctx, int mode, double split_tol);
+
+/* How the FP64 iterations that finish a TSC_SPLIT_BF16 solve stop (no
+ * counterpart in the reference): 0 (at creation) uses the reference's own
+ * stop, successive Ritz values within lanzero (eigen.f90:101), from the split
+ * solve's vector; residual_factor > 0 stops instead when the FP64 Ritz
+ * residual ||H psi - E psi|| is <= residual_factor * sqrt(lanzero) (tighter
+ * and costlier: 0.1 takes ~4x the FP64 iterations on a YC4x12 sweep). */
+int tsc_set_split_refinement(tsc_ctx* ctx, double residual_factor);
 
 /* Pre-sliced operand views of the current superblock's split-precision task
  * lists (no counterpart in the reference): bytes[0..2] and views[0..2] for the

@@ -21,7 +21,7 @@ EXPORTED = [
     "tsc_renormalize", "tsc_wave_transform", "tsc_dmrg_run", "tsc_set_capture", "tsc_get_capture",
     "tsc_hpsi_stats", "tsc_stream", "tsc_hpsi_noalloc", "tsc_set_precision", "tsc_set_split_wait_limit",
     "tsc_set_resident_limit", "tsc_spill_stats", "tsc_split_views",
-    "tsc_checkpoint_write", "tsc_checkpoint_read",
+    "tsc_checkpoint_write", "tsc_checkpoint_read", "tsc_set_split_refinement",
     "tsc_blocksparse_set", "tsc_blocksparse_apply", "tsc_measure_density", "tsc_measure_density_cor", "tsc_set_autotune",
     "tsc_autotune_table", "tsc_autotune_superblock",
 ]
@@ -93,6 +93,7 @@ def load():
     L.tsc_set_resident_limit.argtypes = [c_void, c_ll]
     L.tsc_split_views.argtypes = [c_void, P(c_ll), P(c_int)]
     L.tsc_checkpoint_write.argtypes = [c_void, ctypes.c_char_p]
+    L.tsc_set_split_refinement.argtypes = [c_void, c_double]
     L.tsc_checkpoint_read.argtypes = [c_void, ctypes.c_char_p]
     L.tsc_spill_stats.argtypes = [c_void, P(c_ll), P(c_ll), P(c_double), P(c_double), P(c_ll), P(c_ll)]
     L.tsc_blocksparse_set.argtypes = [c_void, c_int, ctypes.POINTER(c_int), c_ll, ctypes.POINTER(c_double), c_ll,

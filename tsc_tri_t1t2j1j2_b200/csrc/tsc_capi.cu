@@ -381,6 +381,14 @@ int tsc_set_precision(tsc_ctx* ctx, int mode, double split_tol) {
   });
 }
 
+int tsc_set_split_refinement(tsc_ctx* ctx, double residual_factor) {
+  return guard(ctx, [&] {
+    if (!ctx->eng) throw Error(TSC_E_STATE, "no engine");
+    if (!(residual_factor >= 0.0)) throw Error(TSC_E_ARG, "residual factor must be >= 0");
+    ctx->eng->refine_res_ = residual_factor;
+  });
+}
+
 int tsc_set_split_wait_limit(tsc_ctx* ctx, long long polls) {
   return guard(ctx, [&] {
     if (!ctx->eng) throw Error(TSC_E_STATE, "no engine");

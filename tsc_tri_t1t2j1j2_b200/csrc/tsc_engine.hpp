@@ -313,6 +313,10 @@ class Engine {
   // superblock set on.
   int precision_ = 0;
   double split_tol_ = 1e-9;   // relative Ritz-value change that ends the split iterations
+  // FP64 iterations that finish a split solve stop when the Ritz residual is
+  // <= refine_res_ * sqrt(lanzero); 0 (the default): the reference's own stop
+  // (successive Ritz values within lanzero, eigen.f90:101)
+  double refine_res_ = 0.0;
   bool split_now_ = false;    // the current superblock's solve uses the split form
   bool in_warmup_ = false;    // set while the warm-up (infinite-lattice) steps run
 

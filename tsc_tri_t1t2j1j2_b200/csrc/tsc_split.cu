@@ -30,8 +30,8 @@
 // that complete on the stage's full barrier; one lane of the MMA warp issues
 // the step's 24 MMAs into one of two TMEM accumulators and commits them to the
 // stage's empty barrier (and, after a segment's last step, to the
-// accumulator's full barrier); 4 epilogue warps drain the other accumulator
-// into the tile in FP64 (the first segment with beta and the element terms,
+// accumulator's full barrier); 8 epilogue warps (two per TMEM lane quadrant,
+// 32 columns each) drain the other accumulator into the tile in FP64 (the first segment with beta and the element terms,
 // later ones adding to it) while the next segment runs.
 // Every mbarrier wait is bounded (wait_limit polls, a launch argument): on
 // timeout the kernel raises a CTA abort flag and the caller's fault word, waits
@@ -47,8 +47,9 @@ namespace tsc {
 namespace {
 
 constexpr int SP_TM = 128, SP_TN = 64, SP_TK = 16, SP_STAGES = 5;
-constexpr int SP_PRODUCER_WARP = 0, SP_MMA_WARP = 1;            // warps 2..5: epilogue
-constexpr int SP_THREADS = 6 * 32;
+constexpr int SP_PRODUCER_WARP = 0, SP_MMA_WARP = 1;            // warps 2..9: epilogue
+constexpr int SP_EPI_WARPS = 8;   // two per TMEM lane quadrant, each draining 32 of the tile's 64 columns
+constexpr int SP_THREADS = (2 + SP_EPI_WARPS) * 32;
 constexpr int A_PLANE = SP_TM * SP_TK * 2;                     // bytes of one BF16 plane of A
 constexpr int B_PLANE = SP_TN * SP_TK * 2;                     // ... of B
 constexpr int STAGE_BYTES = 6 * A_PLANE + 6 * B_PLANE;         // 36,864
@@ -278,7 +279,7 @@ grouped_zgemm_split_kernel(const GJob* __restrict__ jobs, int njobs, const GGrou
     }
     for (int a = 0; a < 2; ++a) {
       asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&accf[a])) : "memory");
-      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&acce[a])), "r"(4) : "memory");
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&acce[a])), "r"(SP_EPI_WARPS) : "memory");
     }
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(fin)) : "memory");
     *abort_flag = 0;
@@ -404,6 +405,7 @@ grouped_zgemm_split_kernel(const GJob* __restrict__ jobs, int njobs, const GGrou
   } else {
     // ---------------------------------------------------------------- epilogue
     const int quad = warp & 3;               // TMEM lane quadrant this warp may read
+    const int cb0 = ((warp - 2) >> 2) * (SP_TN / 16);   // its half of the tile's 8-column chunks
     int sg = 0;
     bool ok = true;
     for (int jb = blockIdx.x; jb < njobs && ok; jb += gridDim.x) {
@@ -435,7 +437,7 @@ grouped_zgemm_split_kernel(const GJob* __restrict__ jobs, int njobs, const GGrou
         }
         const uint32_t lane_base = tmem + a * (4 * SP_TN) + ((uint32_t)(quad * 32) << 16);
 #pragma unroll 1
-        for (int cb = 0; cb < SP_TN / 8; ++cb) {
+        for (int cb = cb0; cb < cb0 + SP_TN / 16; ++cb) {
           const int c0 = cb * 8;
           double cr[8], ci[8];
           __syncwarp();
@@ -454,7 +456,7 @@ grouped_zgemm_split_kernel(const GJob* __restrict__ jobs, int njobs, const GGrou
 #pragma unroll
             for (int j = 0; j < 8; ++j) cr[j] = ci[j] = 0.0;
           }
-          if (nseg > 0 && cb == SP_TN / 8 - 1) {   // accumulator read out: hand it back
+          if (nseg > 0 && cb == cb0 + SP_TN / 16 - 1) {   // its part of the accumulator read out: hand it back
             fence_before_sync();
             __syncwarp();
             if (lane == 0) mbar_arrive(smem_u32(&acce[a]));

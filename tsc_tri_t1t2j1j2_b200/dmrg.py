@@ -112,6 +112,11 @@ class Context:
         superblock set."""
         self._check(self.L.tsc_set_precision(self.h, int(mode), float(split_tol)))
 
+    def set_split_refinement(self, residual_factor: float):
+        """FP64 finish of split solves: stop at residual <= factor * sqrt(lanzero)
+        (0.1 by default); 0 = the reference's stop (Ritz values within lanzero)."""
+        self._check(self.L.tsc_set_split_refinement(self.h, float(residual_factor)))
+
     def set_split_wait_limit(self, polls: int):
         """Poll limit of the split kernel's bounded waits (default 1<<20; 0 makes
         every wait give up at once, so the next split call fails with TSC_E_CUDA)."""
