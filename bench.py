@@ -343,6 +343,8 @@ def split_leg(torch, dev, sb, steps, fp64_out, model=MODEL, fp64_ms=None):
 
 
 SWEEP_CONFIG = dict(kept_min=200, kept_warm=200, sweeps=[200, 400, 600, 800, 1000, 1000], lanzero=1e-10)
+SWEEP_WORKLOAD = ("YC4x12 t1=1 t2=0.3 J1=0.4 J2=0.036, warm-up m=200, 6 sweeps m=200,400,600,800,1000,1000, "
+                  "lanzero 1e-10, random start seed 1")
 
 
 def sweep_leg(dev):
@@ -350,8 +352,7 @@ def sweep_leg(dev):
     on the device in both forms: seconds of the warm-up and of the sweeps, the
     final energies and their relative difference."""
     from tsc_tri_t1t2j1j2_b200 import Context
-    res = {"workload": "YC4x12 t1=1 t2=0.3 J1=0.4 J2=0.036, warm-up m=200, 6 sweeps m=200,400,600,800,1000,1000, "
-                       "lanzero 1e-10, random start seed 1"}
+    res = {"workload": SWEEP_WORKLOAD}
     for name, mode in (("fp64", Context.FP64), ("split", Context.SPLIT_BF16)):
         ctx = Context(device=dev.index, **MODEL)
         ctx.set_precision(mode, 1e-11)
@@ -679,6 +680,76 @@ def traffic_model(sb):
     return 16 * (int(off) + 2 * int(n))
 
 
+def dmrg_steps(args):
+    """Config 3 whole DMRG steps in both forms: YC4x24, warm-up to m=4000 (FP64 in
+    both forms, the reference's warm-up tolerance 1e-3), then the first
+    `--dmrg-steps` steps of the following half sweep at lanzero 1e-10, once with
+    the plain FP64 form and once with the split form.  Prints one JSON line with
+    the seconds of every step (and of its Lanczos solve), iteration counts,
+    energies and the split form's per-step |dE/E| against FP64.  Not a bench
+    line: about 30 GPU-minutes."""
+    from tsc_tri_t1t2j1j2_b200 import Context
+    N = MODEL3["Nx"] * MODEL3["Ny"]
+    nwarm = N // 2 - 1
+    res = {"workload": f"YC4x24 warm-up to m=4000 (lanzero 1e-3) + {args.dmrg_steps} steps of the first half sweep "
+                       "at m=4000, lanzero 1e-10", "forms": {}}
+    forms = [f for f in (("fp64", Context.FP64), ("split", Context.SPLIT_BF16)) if f[0] in args.dmrg_forms.split(",")]
+    for name, mode in forms:
+        ctx = Context(device=0, **MODEL3)
+        ctx.set_precision(mode, 1e-11)
+        t0 = time.perf_counter()
+        st = ctx.get_ground_state(4000, 4000, [4000], lanzero=1e-10, seed=1, max_solves=nwarm + args.dmrg_steps,
+                                  lanzero_warmup=1e-3)
+        wall = time.perf_counter() - t0
+        spill = ctx.spill_stats()
+        ctx.close()
+        keys = ("phase", "sys_len", "e0", "lanczos_iters", "split_iters", "num_state", "trun_err", "step_seconds",
+                "lanczos_seconds", "hpsi_seconds", "set_seconds", "truncate_seconds", "grow_seconds", "wave_seconds")
+        res["forms"][name] = {"wall_seconds": wall, "warmup_seconds": sum(x["step_seconds"] for x in st[:nwarm]),
+                              "spill": spill, "steps": [{k: x[k] for k in keys} for x in st[nwarm:]]}
+        print(name, wall, flush=True, file=sys.stderr)
+    res["step_seconds"] = {k: sum(x["step_seconds"] for x in v["steps"]) for k, v in res["forms"].items()}
+    if len(res["forms"]) == 2:
+        a, b = res["forms"]["fp64"]["steps"], res["forms"]["split"]["steps"]
+        res["dE_over_E_split_vs_fp64"] = [abs(x["e0"] - y["e0"]) / abs(x["e0"]) for x, y in zip(a, b)]
+        res["steps_speedup_split_over_fp64"] = res["step_seconds"]["fp64"] / res["step_seconds"]["split"]
+    print(json.dumps(res), flush=True)
+    return 0
+
+
+def sweep_study(args):
+    """The YC4x12 whole run of the sweep leg four ways: FP64 at lanzero 1e-13 (the
+    converged reference energy), the split form with the reference's stop for its
+    FP64 finish, the split form with the residual stop 0.1 sqrt(lanzero), and
+    FP64 at lanzero 1e-10.  Prints one JSON line: seconds, iterations and each
+    final energy's distance from the FP64 and the converged runs."""
+    from tsc_tri_t1t2j1j2_b200 import Context
+    runs = (("fp64_lanzero_1e-13", Context.FP64, 1e-13, None), ("split_reference_stop", Context.SPLIT_BF16, 1e-10, 0.0),
+            ("split_residual_0.1", Context.SPLIT_BF16, 1e-10, 0.1), ("fp64", Context.FP64, 1e-10, None))
+    out = {"workload": SWEEP_WORKLOAD}
+    for name, mode, lz, refine in runs:
+        ctx = Context(device=0, **MODEL)
+        ctx.set_precision(mode, 1e-11)
+        if refine is not None:
+            ctx.set_split_refinement(refine)
+        t0 = time.perf_counter()
+        st = ctx.get_ground_state(**dict(SWEEP_CONFIG, lanzero=lz))
+        wall = time.perf_counter() - t0
+        ctx.close()
+        sw = [x for x in st if x["phase"] != 0]
+        out[name] = {"wall_seconds": wall, "sweep_seconds": sum(x["step_seconds"] for x in sw),
+                     "lanczos_seconds": sum(x["lanczos_seconds"] for x in sw),
+                     "lanczos_iters": int(sum(x["lanczos_iters"] for x in sw)),
+                     "split_iters": int(sum(x["split_iters"] for x in sw)), "final_e0": st[-1]["e0"]}
+    t, f = out["fp64_lanzero_1e-13"]["final_e0"], out["fp64"]["final_e0"]
+    for name, *_ in runs:
+        e = out[name]["final_e0"]
+        out[name]["dE_over_E_vs_fp64"] = abs(e - f) / abs(f)
+        out[name]["dE_over_E_vs_converged"] = abs(e - t) / abs(t)
+    print(json.dumps(out), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -692,7 +763,16 @@ def main():
                     help="headline superblock: 3 = YC4x24 m=4000 (default), 2 = YC4x12 m=1000")
     ap.add_argument("--scale", type=int, default=1,
                     help="multiply every dimension of the superblock by this (4: m ~ 4000 size class)")
+    ap.add_argument("--sweep-study", action="store_true",
+                    help="instead of the bench line: the YC4x12 whole run in four solver settings")
+    ap.add_argument("--dmrg-steps", type=int, default=0,
+                    help="instead of the bench line: config-3 warm-up + this many m=4000 DMRG steps in both forms")
+    ap.add_argument("--dmrg-forms", default="fp64,split", help="forms run by --dmrg-steps (comma-separated)")
     args = ap.parse_args()
+    if args.dmrg_steps > 0:
+        return dmrg_steps(args)
+    if args.sweep_study:
+        return sweep_study(args)
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":

@@ -59,6 +59,9 @@ typedef struct tsc_sweep_config {
   int resume;              /* 1: skip the warm-up and the two half sweeps and run the sweeps
                             * from the state tsc_checkpoint_read loaded (the reference's
                             * restart1 = 1 from restart.dat, main.f90:36-38, 147-174) */
+  int max_solves;          /* > 0: stop the run after this many Lanczos solves (DMRG steps);
+                            * 0: run the whole schedule */
+  double lanzero_warmup;   /* > 0: Lanczos tolerance of the warm-up steps alone (else as lanzero) */
 } tsc_sweep_config;
 
 /* One record per Lanczos solve (eigen.f90:169-173, den_mat.f90:342-350). */
@@ -184,6 +187,25 @@ int tsc_measure_density(tsc_ctx* ctx, double* out, int nsites);
  * Nx*Ny values, out[j-1] = Re <n_site n_j> for those j and 0 elsewhere (as the
  * reference's zero-initialised correlation matrix row); returns Nx*Ny. */
 int tsc_measure_density_cor(tsc_ctx* ctx, int site, double* out, int nsites);
+
+/* The three two-site correlations main.f90 measures with Get_density_cor
+ * (measure.f90:2525-2681), selected by kind:
+ *   TSC_COR_DENSITY   <n_site n_j>            (num_elec, Flags 'B'; main.f90:299)
+ *   TSC_COR_SPIN      <S_site . S_j>          (st_sd x st_sd, Flags 'B', rank 1; main.f90:275)
+ *   TSC_COR_ELECTRON  sum_s <c+_site,s c_j,s> (st_elec_up x st_elec_down, Flags 'F',
+ *                                              rank 1/2; main.f90:288)
+ * Operators of nonzero rank travel into the blocks by the reference's ndia
+ * transport (Get_sys_oper_ndia / Change_sys_oper_ndia, get_sys.f90:1536-1723),
+ * results carry the reference's scale sqrt(1+K)*(K==2 ? -1 : 1)
+ * (measure.f90:2586-2587).  Same site range and partners as
+ * tsc_measure_density_cor; out holds 2*nsites doubles, the complex value of
+ * partner j as out[2(j-1)] (real) and out[2(j-1)+1] (imaginary), as main.f90
+ * writes both parts (main.f90:282, 294); the density kind's imaginary part is
+ * written as 0.  Returns Nx*Ny. */
+#define TSC_COR_DENSITY 0
+#define TSC_COR_SPIN 1
+#define TSC_COR_ELECTRON 2
+int tsc_measure_correlation(tsc_ctx* ctx, int kind, int site, double* out, int nsites);
 
 /* Checkpoint in the reference's file format (names dmrg_sub.f90:657-709):
  * writes into directory dir, for every model, truncation and basis the last

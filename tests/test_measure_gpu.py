@@ -62,3 +62,41 @@ def test_density_cor_matches_oracle(mode, lanzero, tol):
         assert np.count_nonzero(ref[s]) >= 3
         assert np.max(np.abs(got[s] - ref[s])) <= tol, s
         assert np.array_equal(got[s] == 0, ref[s] == 0)
+
+
+def oracle_correlations(lanzero, sites):
+    cfg = orc.RunConfig(Nx=4, Ny=4, t1=1.0, t2=0.3, J1=0.4, J2=0.036, lanzero=lanzero, final_half_sweep=True, **RUN)
+    o = orc.Oracle(cfg)
+    o.run()
+    out = {}
+    for kind, get in (("density", o.density_cor), ("spin", o.spin_cor), ("electron", o.elec_cor)):
+        out[kind] = {s: get(s) for s in sites}
+    return out
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("mode,lanzero,tol", [(Context.FP64, 1e-10, 1e-11), (Context.SPLIT_BF16, 1e-13, 1e-7)])
+def test_spin_and_electron_cor_match_oracle(mode, lanzero, tol):
+    """tsc_measure_correlation for the spin (st_sd x st_sd, rank 1, 'B') and
+    electron (st_elec_up x st_elec_down, rank 1/2, 'F') correlations after the
+    final half sweep, sites 1-4 (partners inside the system block, on its added
+    site, on the environment's added site and inside the environment block),
+    complex, against the oracle's oper_cor, tolerances as for <n_i>; the
+    density kind equals tsc_measure_density_cor."""
+    sites = (1, 2, 3, 4)
+    ref = oracle_correlations(lanzero, sites)
+    ctx = Context(4, 4, 1.0, 0.3, 0.4, 0.036)
+    try:
+        ctx.set_precision(mode, 1e-11)
+        ctx.get_ground_state(lanzero=lanzero, final_half_sweep=True, **RUN)
+        got = {k: {s: ctx.measure_correlation(k, s) for s in sites} for k in ("density", "spin", "electron")}
+        dens = {s: ctx.measure_density_cor(s) for s in sites}
+    finally:
+        ctx.close()
+    for s in sites:
+        assert np.array_equal(got["density"][s].real, dens[s]) and not got["density"][s].imag.any()
+        for kind in ("spin", "electron"):
+            r, g = ref[kind][s], got[kind][s]
+            assert np.count_nonzero(r) >= 3, (kind, s)
+            assert np.max(np.abs(g - r)) <= tol, (kind, s, np.max(np.abs(g - r)))
+            assert np.array_equal(g == 0, r == 0), (kind, s)

@@ -74,15 +74,18 @@ def test_split_full_run_energies():
     Lanczos when successive Ritz values agree to lanzero, which leaves its
     vectors about sqrt(lanzero/gap) from the eigenvector; a different (correct)
     solver then truncates a slightly different basis and the two runs drift
-    apart by ~1e-9 at lanzero = 1e-10.  With lanzero = 1e-13 both runs are
-    converged well below that and the last quarter of the steps agree to
-    better than 1e-10 relative (about 4e-11 measured)."""
+    apart by ~1e-9 at lanzero = 1e-10.  With lanzero = 1e-13 and the split
+    solves finished to a Ritz residual of 0.1*sqrt(lanzero) the last quarter of
+    the steps agree to better than 1e-10 relative (about 4e-11 measured); with
+    the reference's stop for the FP64 finish (the default) the split vector
+    keeps more of its BF16 error and the tail differs by ~2e-10."""
     cfg = orc.RunConfig(Nx=3, Ny=4, t1=1.0, t2=0.3, J1=0.4, J2=0.036, kept_min=40, kept_warm=40, sweeps=[40],
                         lanzero=1e-13)
     ref_steps = orc.Oracle(cfg).run()
     ctx = Context(3, 4, 1.0, 0.3, 0.4, 0.036)
     try:
         ctx.set_precision(SPLIT, 1e-11)
+        ctx.set_split_refinement(0.1)
         steps = ctx.get_ground_state(kept_min=40, kept_warm=40, sweeps=[40], lanzero=1e-13)
     finally:
         ctx.close()

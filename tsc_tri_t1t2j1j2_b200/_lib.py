@@ -22,7 +22,8 @@ EXPORTED = [
     "tsc_hpsi_stats", "tsc_stream", "tsc_hpsi_noalloc", "tsc_set_precision", "tsc_set_split_wait_limit",
     "tsc_set_resident_limit", "tsc_spill_stats", "tsc_split_views",
     "tsc_checkpoint_write", "tsc_checkpoint_read", "tsc_set_split_refinement",
-    "tsc_blocksparse_set", "tsc_blocksparse_apply", "tsc_measure_density", "tsc_measure_density_cor", "tsc_set_autotune",
+    "tsc_blocksparse_set", "tsc_blocksparse_apply", "tsc_measure_density", "tsc_measure_density_cor", "tsc_measure_correlation",
+    "tsc_set_autotune",
     "tsc_autotune_table", "tsc_autotune_superblock",
 ]
 
@@ -35,7 +36,8 @@ class ModelConfig(ctypes.Structure):
 class SweepConfig(ctypes.Structure):
     _fields_ = [("kept_min", c_int), ("kept_max_warmup", c_int), ("nsweeps", c_int),
                 ("sweep_kept_max", P(c_int)), ("lanzero", c_double), ("seed", ctypes.c_ulonglong),
-                ("warmup_only", c_int), ("final_half_sweep", c_int), ("resume", c_int)]
+                ("warmup_only", c_int), ("final_half_sweep", c_int), ("resume", c_int), ("max_solves", c_int),
+                ("lanzero_warmup", c_double)]
 
 
 class StepLog(ctypes.Structure):
@@ -101,6 +103,7 @@ def load():
     L.tsc_blocksparse_apply.argtypes = [c_void, c_void, c_void, c_int]
     L.tsc_measure_density.argtypes = [c_void, ctypes.POINTER(c_double), c_int]
     L.tsc_measure_density_cor.argtypes = [c_void, c_int, ctypes.POINTER(c_double), c_int]
+    L.tsc_measure_correlation.argtypes = [c_void, c_int, c_int, ctypes.POINTER(c_double), c_int]
     L.tsc_set_autotune.argtypes = [c_void, c_int]
     L.tsc_autotune_table.argtypes = [c_void, ctypes.POINTER(c_int), ctypes.POINTER(c_double), c_int]
     L.tsc_autotune_superblock.argtypes = [c_void, c_int]

@@ -6,7 +6,7 @@ import subprocess
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-SRC = ["tsc_kernels.cu", "tsc_host.cu", "tsc_hpsi.cu", "tsc_dmrg.cu", "tsc_capi.cu", "tsc_noalloc.cu", "tsc_split.cu", "tsc_blocksparse.cu", "tsc_measure.cu", "tsc_nullspace.cu", "tsc_checkpoint.cu"]
+SRC = ["tsc_kernels.cu", "tsc_host.cu", "tsc_hpsi.cu", "tsc_dmrg.cu", "tsc_capi.cu", "tsc_noalloc.cu", "tsc_split.cu", "tsc_blocksparse.cu", "tsc_measure.cu", "tsc_nullspace.cu", "tsc_checkpoint.cu", "tsc_correlate.cu"]
 DEPS = SRC + ["tsc_kernels.cuh", "tsc_engine.hpp", "tsc_ctx.hpp"]
 OUT = os.path.join(HERE, "_lib", "libtscgpu.so")
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",

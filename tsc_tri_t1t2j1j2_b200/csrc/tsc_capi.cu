@@ -333,8 +333,9 @@ int tsc_dmrg_run(tsc_ctx* ctx, const tsc_sweep_config* sw, tsc_step_log* log, in
     if (sw->kept_min < 1 || sw->kept_max_warmup < 1) throw Error(TSC_E_ARG, "kept sizes must be positive");
     std::vector<int> sweeps(sw->sweep_kept_max, sw->sweep_kept_max + sw->nsweeps);
     std::vector<Engine::StepRec> recs;
+    ctx->eng->lanzero_warmup_ = sw->lanzero_warmup > 0 ? sw->lanzero_warmup : 0.0;
     ctx->eng->run(sw->kept_min, sw->kept_max_warmup, sweeps, sw->lanzero, sw->seed, &recs, sw->warmup_only != 0,
-                  sw->final_half_sweep != 0, sw->resume != 0);
+                  sw->final_half_sweep != 0, sw->resume != 0, sw->max_solves > 0 ? sw->max_solves : 0);
     nsteps = (int)recs.size();
     for (int i = 0; i < nsteps && i < max_steps && log; ++i) {
       const auto& s = recs[i];

@@ -1255,7 +1255,7 @@ void Engine::warm_up(int end_id, double trun_err, std::vector<StepRec>* log) {
   DModel sys = site_model(), env = site_model();
   models_.put(0, 1, sys);
   models_.put(1, 1, env);
-  while (label + 1 <= end_id) {
+  while (label + 1 <= end_id && !solve_cap_reached()) {
     auto t0 = std::chrono::steady_clock::now();
     Basis sys_bs = get_basis(sys.ham), env_bs = get_basis(env.ham);
     L.setup(sys.ham.len, env.ham.len);
@@ -1329,6 +1329,7 @@ void Engine::warm_up(int end_id, double trun_err, std::vector<StepRec>* log) {
 }
 
 void Engine::left_to_right(int bg_id, int end_id, double trun_err, std::vector<StepRec>* log) {
+  if (solve_cap_reached()) return;   // a capped run stores no models past its last step
   const int N = L.num_site;
   int label = bg_id;
   DModel sys = models_.get(0, label), env = models_.get(1, N - label - 2);
@@ -1338,7 +1339,7 @@ void Engine::left_to_right(int bg_id, int end_id, double trun_err, std::vector<S
   DevBufP psi;
   DBlock sys_trun, env_trun;
   bool first = true;
-  while (true) {
+  while (!solve_cap_reached()) {
     auto t0 = std::chrono::steady_clock::now();
     double wave_s = 0.0;
     if (!first) {
@@ -1395,6 +1396,7 @@ void Engine::left_to_right(int bg_id, int end_id, double trun_err, std::vector<S
 }
 
 void Engine::right_to_left(int bg_id, int end_id, double trun_err, std::vector<StepRec>* log) {
+  if (solve_cap_reached()) return;
   const int N = L.num_site;
   int label = bg_id;
   DModel sys = models_.get(0, label - 1), env = models_.get(1, N - label - 1);
@@ -1404,7 +1406,7 @@ void Engine::right_to_left(int bg_id, int end_id, double trun_err, std::vector<S
   DevBufP psi;
   DBlock sys_trun, env_trun;
   bool first = true;
-  while (true) {
+  while (!solve_cap_reached()) {
     auto t0 = std::chrono::steady_clock::now();
     double wave_s = 0.0;
     if (!first) {
@@ -1461,7 +1463,9 @@ void Engine::right_to_left(int bg_id, int end_id, double trun_err, std::vector<S
 }
 
 void Engine::run(int kept_min, int kept_warm, const std::vector<int>& sweeps, double lanzero_override,
-                 unsigned long long seed, std::vector<StepRec>* log, bool warmup_only, bool final_half, bool resume) {
+                 unsigned long long seed, std::vector<StepRec>* log, bool warmup_only, bool final_half, bool resume,
+                 int max_solves) {
+  max_solves_ = max_solves;
   const int N = L.num_site;
   rng = seed;
   nsolve_ = 0;
@@ -1482,7 +1486,7 @@ void Engine::run(int kept_min, int kept_warm, const std::vector<int>& sweeps, do
     sys_bsm.clear();
     env_bsm.clear();
     restart1 = 0;
-    lanzero_ = lz(lanerr * 1000);
+    lanzero_ = lanzero_warmup_ > 0 ? lanzero_warmup_ : lz(lanerr * 1000);
     warm_up(N / 2, trun_err * 100, log);
     if (warmup_only) return;
     lanzero_ = lz(lanerr * 15);

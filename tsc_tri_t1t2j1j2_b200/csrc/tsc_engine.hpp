@@ -142,6 +142,7 @@ struct Lattice {
 };
 
 double w6j(int j1, int j2, int j3, int l1, int l2, int l3);   // doubled arguments
+double w3j(int j1, int j2, int j3, int m1, int m2, int m3);   // doubled arguments
 
 // ---- task lists -------------------------------------------------------------------
 struct TaskList {
@@ -307,7 +308,22 @@ class Engine {
   DBlock site_dia(const SiteOp& so, const Basis& basis);
   DBlock block_dia(const DBlock& blk, const Basis& basis);
   DBlock trun_dia(const DBlock& ori, const DBlock& trun);
-  double expect_dia(const DBlock* bl, const SiteOp* so, const Basis& bs, bool sys);
+  double expect_dia(const DBlock* bl, const SiteOp* so, const Basis& bs, bool sys, double* imag = nullptr);
+  // <op1_site op2_j> for operators of any rank (Get_density_cor, tsc_correlate.cu)
+  std::vector<cplx> measure_oper_cor(const SiteOp& op1, const SiteOp& op2, char flag, int site);
+  DBlock ndia_layout(const Basis& basis, int up_dif, int K, TaskList& tl, std::vector<int>& g);
+  DBlock site_ndia(const SiteOp& so, const Basis& basis, bool env, char flag);
+  DBlock block_ndia(const DBlock& blk, const Basis& basis, bool env, char flag);
+  DBlock trun_ndia(const DBlock& ori, const DBlock& trun);
+  DBlock oper_ndia_in_block(const SiteOp& so, int old_idx, int new_idx, bool sys, bool trunc, char flag);
+  DBlock carry_ndia(const DBlock& op, int from, int to, bool sys, char flag);
+  DBlock product_to_scalar(const DBlock& o1, const DBlock& o2, const Basis& basis);
+  DBlock transfer_trans(const DBlock& in);
+  struct PairSum;
+  cplx pair_sum(PairSum& ps);
+  cplx corr_site_ndia(const DBlock& bl, const SiteOp& st_op, const Basis& bs, char flag);
+  cplx corr_env_site_ndia(const DBlock& bl, const SiteOp& est, const Basis& sbs, const Basis& ebs, char flag);
+  cplx corr_env_block_ndia(const DBlock& bl, const DBlock& ebl, const Basis& sbs, const Basis& ebs, char flag);
   // 0: complex FP64 throughout; 1: H.psi sector GEMMs as BF16 slices on the
   // tensor cores, Lanczos finished by FP64 iterations.  Applies from the next
   // superblock set on.
@@ -395,7 +411,11 @@ class Engine {
   // sweeps from the state checkpoint_read loaded (restart1 = 1, main.f90:36-38)
   void run(int kept_min, int kept_warm, const std::vector<int>& sweeps, double lanzero_override,
            unsigned long long seed, std::vector<StepRec>* log, bool warmup_only = false, bool final_half = false,
-           bool resume = false);
+           bool resume = false, int max_solves = 0);
+  // a run stops once it has made max_solves_ Lanczos solves (0: no cap)
+  int max_solves_ = 0;
+  double lanzero_warmup_ = 0.0;   // > 0: the warm-up's Lanczos tolerance (else the run's)
+  bool solve_cap_reached() const { return max_solves_ > 0 && nsolve_ >= max_solves_; }
   // the reference's checkpoint files (tsc_checkpoint.cu): every stored model,
   // truncation and basis of the last run and its last wavefunction
   int checkpoint_write(const std::string& dir);

@@ -206,6 +206,32 @@ double w6j(int j1, int j2, int j3, int l1, int l2, int l3) {
   return omega * std::sqrt(th);
 }
 
+// Wigner 3j symbol with doubled arguments by Racah's single-sum formula
+// (the reference's W3JS, block.f90:3702-3741, evaluates the same sum):
+// (-1)^(j1-j2-m3) sqrt(D(j1 j2 j3) prod (j+-m)!) sum_k (-1)^k / [k! (j3-j2+m1+k)!
+// (j3-j1-m2+k)! (j1+j2-j3-k)! (j1-m1-k)! (j2+m2-k)!]
+double w3j(int j1, int j2, int j3, int m1, int m2, int m3) {
+  const double* f = factorials();
+  if (m1 + m2 + m3 != 0) return 0.0;
+  if (j3 > j1 + j2 || j3 < std::abs(j1 - j2)) return 0.0;
+  if (((j1 + j2 + j3) & 1) || ((j1 - m1) & 1) || ((j2 - m2) & 1)) return 0.0;
+  if (std::abs(m1) > j1 || std::abs(m2) > j2 || std::abs(m3) > j3) return 0.0;
+  // k in doubled units
+  const int klo = std::max(0, std::max(j2 - j3 - m1, j1 - j3 + m2));
+  const int khi = std::min(j1 + j2 - j3, std::min(j1 - m1, j2 + m2));
+  double sum = 0.0;
+  for (int k = klo; k <= khi; k += 2) {
+    double den = f[k / 2] * f[(j3 - j2 + m1 + k) / 2] * f[(j3 - j1 - m2 + k) / 2] * f[(j1 + j2 - j3 - k) / 2] *
+                 f[(j1 - m1 - k) / 2] * f[(j2 + m2 - k) / 2];
+    sum += (k % 4 == 0) ? 1.0 / den : -1.0 / den;
+  }
+  const double tri = f[(j1 + j2 - j3) / 2] * f[(j1 - j2 + j3) / 2] * f[(-j1 + j2 + j3) / 2] / f[(j1 + j2 + j3) / 2 + 1];
+  const double mf = f[(j1 + m1) / 2] * f[(j1 - m1) / 2] * f[(j2 + m2) / 2] * f[(j2 - m2) / 2] * f[(j3 + m3) / 2] *
+                    f[(j3 - m3) / 2];
+  const double v = sum * std::sqrt(tri * mf);
+  return (((j1 - j2 - m3) / 2) % 2 != 0) ? -v : v;
+}
+
 // ---- lattice (dmrg_sub.f90:304-644) -------------------------------------------------
 void Lattice::init(int nx, int ny, double t1, double t2, double J1, double J2, int oy) {
   Nx = nx;

@@ -312,6 +312,40 @@ __global__ void multi_dot_partial(const double2* __restrict__ X, long long ld, i
   }
 }
 
+// partial sums of <x, y> = sum conj(x) y: real parts at partial[b], imaginary at partial[nblk + b]
+__global__ void zdot_partial(const double2* __restrict__ x, const double2* __restrict__ y, long long n,
+                             double* __restrict__ partial, int nblk) {
+  __shared__ double red[2][VB / 32];
+  const long long beg = (long long)blockIdx.x * VCHUNK;
+  const long long end = beg + VCHUNK < n ? beg + VCHUNK : n;
+  double ar = 0.0, ai = 0.0;
+  for (long long e = beg + threadIdx.x; e < end; e += VB) {
+    const double2 a = x[e], b = y[e];
+    ar = fma(a.x, b.x, ar);
+    ar = fma(a.y, b.y, ar);
+    ai = fma(a.x, b.y, ai);
+    ai = fma(-a.y, b.x, ai);
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    ar += __shfl_xor_sync(0xffffffffu, ar, o);
+    ai += __shfl_xor_sync(0xffffffffu, ai, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    red[0][threadIdx.x >> 5] = ar;
+    red[1][threadIdx.x >> 5] = ai;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double sr = 0.0, si = 0.0;
+    for (int w = 0; w < VB / 32; ++w) {
+      sr += red[0][w];
+      si += red[1][w];
+    }
+    partial[blockIdx.x] = sr;
+    partial[nblk + blockIdx.x] = si;
+  }
+}
+
 __global__ void multi_dot_final(const double* __restrict__ partial, int nblk, int nvec, double* __restrict__ out) {
   int j = blockIdx.x;
   if (j >= nvec) return;
@@ -634,6 +668,15 @@ cudaError_t launch_multi_dot(const double2* X, long long ld, int nvec, const dou
   if (nblk < 1) nblk = 1;
   multi_dot_partial<<<nblk, VB, 0, st>>>(X, ld, nvec, y, n, partial, nblk);
   multi_dot_final<<<nvec, 256, 0, st>>>(partial, nblk, nvec, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_zdot(const double2* x, const double2* y, long long n, double* partial, double* out,
+                        cudaStream_t st) {
+  int nblk = (int)((n + VCHUNK - 1) / VCHUNK);
+  if (nblk < 1) nblk = 1;
+  zdot_partial<<<nblk, VB, 0, st>>>(x, y, n, partial, nblk);
+  multi_dot_final<<<2, 256, 0, st>>>(partial, nblk, 2, out);
   return cudaGetLastError();
 }
 

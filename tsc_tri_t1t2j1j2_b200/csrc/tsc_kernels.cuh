@@ -133,6 +133,10 @@ cudaError_t launch_reduce_partials(const GReduce* reds, int nred, const GGroup* 
 // partial sums of Re<x_j, y> for j < nvec (x_j = X + j*ld), deterministic two-pass
 cudaError_t launch_multi_dot(const double2* X, long long ld, int nvec, const double2* y, long long n,
                              double* partial, double* out, cudaStream_t st);
+// <x, y> = sum conj(x) y into out[0] (real), out[1] (imaginary); partial holds
+// 2 * ceil(n / 8192) doubles; deterministic two-pass
+cudaError_t launch_zdot(const double2* x, const double2* y, long long n, double* partial, double* out,
+                        cudaStream_t st);
 cudaError_t launch_lanczos_update(double2* w, const double2* v, const double2* vprev, const double* alpha,
                                   const double* beta_prev, long long n, cudaStream_t st);
 cudaError_t launch_scale(double2* w, const double* norm2, long long n, int invert_sqrt, cudaStream_t st);

@@ -207,8 +207,9 @@ DBlock Engine::oper_dia_in_block(const SiteOp& so, int old_idx, int new_idx, boo
 }
 
 // Re <psi | (O x 1) | psi> (sys) or Re <psi | (1 x O) | psi> (env) for a block
-// operator `bl`, or for the site operator `so` on the block's added site.
-double Engine::expect_dia(const DBlock* bl, const SiteOp* so, const Basis& bs, bool sys) {
+// operator `bl`, or for the site operator `so` on the block's added site; the
+// imaginary part into *imag when given.
+double Engine::expect_dia(const DBlock* bl, const SiteOp* so, const Basis& bs, bool sys, double* imag) {
   const WLayout& w = disk_layout;
   const long long n = w.dim;
   DevBuf M((size_t)std::max<long long>(n, 1), st, false);
@@ -271,11 +272,11 @@ double Engine::expect_dia(const DBlock* bl, const SiteOp* so, const Basis& bs, b
   }
   tl.upload(st);
   run_tasks(tl, disk_wave->p, M.p, nullptr);
-  DevBuf part((size_t)((n + 8191) / 8192 + 2) / 2 + 1, st, false);
-  cuda_check(launch_multi_dot(disk_wave->p, 0, 1, M.p, n, reinterpret_cast<double*>(part.p), d_scal + S_MEAS, st),
-             "dot");
-  cuda_check(cudaMemcpyAsync(h_scal + S_MEAS, d_scal + S_MEAS, sizeof(double), cudaMemcpyDeviceToHost, st), "d2h");
+  DevBuf part((size_t)((n + 8191) / 8192 + 1), st, false);
+  cuda_check(launch_zdot(disk_wave->p, M.p, n, reinterpret_cast<double*>(part.p), d_scal + S_MEAS, st), "dot");
+  cuda_check(cudaMemcpyAsync(h_scal + S_MEAS, d_scal + S_MEAS, 2 * sizeof(double), cudaMemcpyDeviceToHost, st), "d2h");
   cuda_check(cudaStreamSynchronize(st), "sync");
+  if (imag) *imag = h_scal[S_MEAS + 1];
   return h_scal[S_MEAS];
 }
 

@@ -113,8 +113,9 @@ class Context:
         self._check(self.L.tsc_set_precision(self.h, int(mode), float(split_tol)))
 
     def set_split_refinement(self, residual_factor: float):
-        """FP64 finish of split solves: stop at residual <= factor * sqrt(lanzero)
-        (0.1 by default); 0 = the reference's stop (Ritz values within lanzero)."""
+        """FP64 finish of split solves: stop at residual <= factor * sqrt(lanzero);
+        0 (the default) = the reference's stop (successive Ritz values within
+        lanzero, eigen.f90:101)."""
         self._check(self.L.tsc_set_split_refinement(self.h, float(residual_factor)))
 
     def set_split_wait_limit(self, polls: int):
@@ -259,13 +260,17 @@ class Context:
 
     # ------------------------------------------------------------------ full run
     def get_ground_state(self, kept_min, kept_warm, sweeps, lanzero=-1.0, seed=1, capture_step=-1, max_steps=100000,
-                         warmup_only=False, final_half_sweep=False, resume=False):
+                         warmup_only=False, final_half_sweep=False, resume=False, max_solves=0,
+                         lanzero_warmup=-1.0):
         """Get_Ground_State (main.f90:114-209); resume=True continues with the sweeps
-        from the state checkpoint_read loaded (no warm-up, no first half sweeps)."""
+        from the state checkpoint_read loaded (no warm-up, no first half sweeps);
+        max_solves > 0 stops the run after that many DMRG steps; lanzero_warmup > 0
+        sets the warm-up's tolerance alone."""
         self._check(self.L.tsc_set_capture(self.h, capture_step))
         sk = (ctypes.c_int * max(1, len(sweeps)))(*sweeps)
         cfg = _lib.SweepConfig(kept_min, kept_warm, len(sweeps), sk, lanzero, seed, 1 if warmup_only else 0,
-                               1 if final_half_sweep else 0, 1 if resume else 0)
+                               1 if final_half_sweep else 0, 1 if resume else 0, int(max_solves),
+                               float(lanzero_warmup))
         logs = (_lib.StepLog * max_steps)()
         n = self._check(self.L.tsc_dmrg_run(self.h, ctypes.byref(cfg), logs, max_steps))
         out = []
@@ -292,6 +297,25 @@ class Context:
         self._check(self.L.tsc_measure_density_cor(self.h, int(site),
                                                    out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), len(out)))
         return out
+
+    # kinds of measure_correlation (TSC_COR_* in include/tsc_gpu.h)
+    COR_KINDS = {"density": 0, "spin": 1, "electron": 2}
+
+    def measure_correlation(self, kind, site=None):
+        """Row `site` of one of the three correlation matrices main.f90 writes
+        (Get_density_cor, measure.f90:2525-2681): "density" <n_site n_j>
+        (main.f90:299), "spin" <S_site . S_j> (st_sd x st_sd, Flags 'B',
+        main.f90:275) or "electron" sum_s <c+_site,s c_j,s> (st_elec_up x
+        st_elec_down, Flags 'F', main.f90:288), complex as the reference writes
+        them (main.f90:282, 294; the density kind's imaginary part is 0).  Same
+        site default, partners and layout as measure_density_cor."""
+        if site is None:
+            site = (self.Nx // 4) * self.Ny + 2 - self.Ny
+        n = self.Nx * self.Ny
+        out = np.zeros(2 * n, dtype=np.float64)
+        self._check(self.L.tsc_measure_correlation(self.h, self.COR_KINDS[kind], int(site),
+                                                   out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), n))
+        return out[0::2] + 1j * out[1::2]
 
     def capture(self):
         ti, tn, td, tc = P(ctypes.c_int)(), ctypes.c_longlong(), P(ctypes.c_double)(), ctypes.c_longlong()
