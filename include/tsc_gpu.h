@@ -62,6 +62,8 @@ typedef struct tsc_sweep_config {
   int max_solves;          /* > 0: stop the run after this many Lanczos solves (DMRG steps);
                             * 0: run the whole schedule */
   double lanzero_warmup;   /* > 0: Lanczos tolerance of the warm-up steps alone (else as lanzero) */
+  int final_stop;          /* > 0: last label of the final half sweep (0: the reference's
+                            * 5*Num_site/6 - 1, main.f90:205-206) */
 } tsc_sweep_config;
 
 /* One record per Lanczos solve (eigen.f90:169-173, den_mat.f90:342-350). */
@@ -131,6 +133,27 @@ int tsc_truncate(tsc_ctx* ctx, int side, const double* psi, int kept_min, int ke
                  const double** trun_data, long long* ntrun_cplx, double* spectrum,
                  long long spectrum_cap);
 
+/* The two halves of tsc_truncate as the reference calls them.
+ * tsc_density_matrix: Get_density_matrix_sys_new (side 0, den_mat.f90:103-138) /
+ * Get_density_matrix_env_new (side 1, den_mat.f90:143-177) on the current
+ * superblock.  psi holds min(levels, 2) waves one after the other (host buffer,
+ * tsc_superblock_dim() elements each): levels = 1 takes the normalised wave;
+ * levels >= 2 averages the density matrices of the first two waves,
+ * unnormalised, as the reference does.  The density matrix (one square
+ * sub-block per wave sector, the reference's sys_den / env_den) is returned in
+ * the Block layout through *den_ints / *den_data (library-owned, valid until the
+ * next call on ctx).
+ * tsc_truncation_operator: Get_truncation_operator (den_mat.f90:190-418) on a
+ * density matrix given in the Block layout (square sub-blocks, down_dif 0);
+ * outputs as tsc_truncate. */
+int tsc_density_matrix(tsc_ctx* ctx, int side, const double* psi, int levels, const int** den_ints,
+                       long long* nden_ints, const double** den_data, long long* nden_cplx);
+int tsc_truncation_operator(tsc_ctx* ctx, const int* den_ints, long long nden_ints, const double* den_data,
+                            long long nden_cplx, int kept_min, int kept_max, double trun_err, int* num_state,
+                            double* err, double* entropy, double* entropy_mult, const int** trun_ints,
+                            long long* ntrun_ints, const double** trun_data, long long* ntrun_cplx, double* spectrum,
+                            long long spectrum_cap);
+
 /* Get_Hamiltonian_Sys / Get_Hamiltonian_Env (get_sys.f90:4-592): enlarges the
  * block of the given side with one site (update_block_*, update_site_*,
  * Get_hamiltonian_*) and renormalises every operator with U (update_trun_dia /
@@ -160,8 +183,9 @@ int tsc_dmrg_run(tsc_ctx* ctx, const tsc_sweep_config* sweep, tsc_step_log* log,
  * under this many bytes, and past it the least recently used ones move to host
  * memory and return to the device when the sweep reads them (results are
  * unchanged: the data round-trips exactly).  bytes < 0 (the default): 45 % of
- * the device's memory; 0: every stored model lives in host memory between its
- * uses. */
+ * the device's memory in the FP64 form, 30 % in the split form (whose
+ * pre-sliced operand views need room beside the superblock); 0: every stored
+ * model lives in host memory between its uses. */
 int tsc_set_resident_limit(tsc_ctx* ctx, long long bytes);
 /* Spill counters of the stored models since the context was created: models
  * moved to host memory, models brought back, bytes moved both ways and the wall
@@ -206,6 +230,19 @@ int tsc_measure_density_cor(tsc_ctx* ctx, int site, double* out, int nsites);
 #define TSC_COR_SPIN 1
 #define TSC_COR_ELECTRON 2
 int tsc_measure_correlation(tsc_ctx* ctx, int kind, int site, double* out, int nsites);
+
+/* Singlet pair correlations <O+_(s1 s2) O_(s3 s4)> of the last ground state,
+ * O+_ab = (c+_a,up c+_b,dn - c+_a,dn c+_b,up)/sqrt(2) (Get_mSCOP_Operator_Cor0 with
+ * Flags 'S0' from the label main.f90:259-262 reaches, measure.f90:2683-2834):
+ * first bond (xc1, neib(xc1, ij1)), which must lie in the system block of the
+ * wave; second bonds (s3, neib(s3, 1|3|5)) for s3 = xc1 + Ny + ij, ... up to
+ * xc2 <= Nx*Ny, in the system block (Get_sys_two / Get_sys_two1) and then in the
+ * environment block (Get_SCOP_Operator_Env and the block-block correlator,
+ * value conjugated as the reference writes it).  Record k: bonds[4k..4k+3] =
+ * s1 s2 s3 s4, values[2k], values[2k+1] = real, imaginary part; at most cap
+ * records are written.  Returns the number of records (which may exceed cap). */
+int tsc_measure_pair_correlation(tsc_ctx* ctx, int xc1, int xc2, int ij, int ij1, int* bonds, double* values,
+                                 int cap);
 
 /* Checkpoint in the reference's file format (names dmrg_sub.f90:657-709):
  * writes into directory dir, for every model, truncation and basis the last
@@ -265,9 +302,11 @@ int tsc_set_precision(tsc_ctx* ctx, int mode, double split_tol);
  * and costlier: 0.1 takes ~4x the FP64 iterations on a YC4x12 sweep). */
 int tsc_set_split_refinement(tsc_ctx* ctx, double residual_factor);
 
-/* Pre-sliced operand views of the current superblock's split-precision task
- * lists (no counterpart in the reference): bytes[0..2] and views[0..2] for the
- * operator views (sliced once per superblock, coefficients folded in), the
+/* Pre-sliced operand views of the split-precision task lists of the superblock
+ * or block-sparse batch set last (no counterpart in the reference): bytes[0..2]
+ * and views[0..2] for the operator views (sliced once per superblock; with the
+ * terms' coefficients folded in for a superblock, one view per operator block
+ * for a batch, whose coefficients the kernel applies per term), the
  * input-vector views (sliced on every H.psi) and the phase-1 intermediates.
  * All zero in the FP64 form. */
 int tsc_split_views(tsc_ctx* ctx, long long* bytes, int* views);

@@ -62,6 +62,34 @@ def test_blocksparse_batch(batch, mode, tol):
 
 
 @pytest.mark.gpu
+def test_blocksparse_split_long_terms():
+    """Split form with inner dimensions up to 700 (terms of up to 44 K steps,
+    several accumulator segments each): the kernel breaks segments at every term
+    and applies the term's coefficient in the epilogue (views shared by all terms
+    of an operator); against numpy <= 2e-6 of the largest element, and the
+    sliced operator views are no larger than one copy per operator block."""
+    import torch
+    rng = np.random.default_rng(5)
+    probs = [synthetic(rng, 4, 200, 700, n_left=3, n_right=3, n_terms=12)]
+    x = random_psi(rng, probs)
+    ref = apply_numpy(probs, x)
+    ctx = Context(3, 4)
+    try:
+        ctx.blocksparse_set(probs)
+        xd = torch.from_numpy(x).cuda()
+        yd = torch.empty_like(xd)
+        ctx.blocksparse_apply(xd.data_ptr(), yd.data_ptr(), Context.SPLIT_BF16)
+        torch.cuda.synchronize()
+        assert rel(yd.cpu().numpy(), ref) <= 2e-6
+        P = probs[0]
+        elems = sum(b.size for _, blks in P.left + P.right for b in blks if b is not None)
+        # 12 bytes per complex element in the six BF16 planes, tiles padded to 128 x 16 / 16 x 64
+        assert ctx.split_views()["operators"][0] <= 12 * elems * 2.5
+    finally:
+        ctx.close()
+
+
+@pytest.mark.gpu
 def test_blocksparse_rejects_mismatched_shifts():
     rng = np.random.default_rng(3)
     P = synthetic(rng, 4, 3, 9, n_left=2, n_right=2, n_terms=2, shifts=(0,))

@@ -101,6 +101,37 @@ def test_truncation_matches_oracle(captured):
 
 
 @pytest.mark.gpu
+def test_density_matrix_entry_and_levels(captured):
+    """tsc_density_matrix (Get_density_matrix_*_new) against the oracle's density
+    matrix (<= 1e-13 of its largest element), tsc_truncation_operator on that
+    matrix bit-identical to tsc_truncate, and levels = 2 equal to the average of
+    the two waves' unnormalised density matrices computed in numpy."""
+    cfg, cap, ctx = captured
+    side = 0 if cap["sys_side"] else 1
+    gs = cap["gs"]
+    den = ctx.get_density_matrix(side, gs.vec)
+    ref = {(int(s[0]), int(s[1])): m for s, m in zip(cap["den"].subs, cap["den"].mats)}
+    scale = max(np.max(np.abs(m)) for m in ref.values())
+    assert den.num == len(ref)
+    for sub, m in zip(den.subs, den.mats):
+        assert np.max(np.abs(m - ref[(int(sub[0]), int(sub[1]))])) <= 1e-13 * scale
+    trun_err = 1.0000000036274937e-15
+    r0 = ctx.get_truncation_operator(side, gs.vec, cfg.kept_min, cfg.sweeps[0], trun_err)
+    r1 = ctx.truncation_from_density(den, cfg.kept_min, cfg.sweeps[0], trun_err)
+    assert r1["num_state"] == r0["num_state"] and r1["err"] == r0["err"] and r1["entropy"] == r0["entropy"]
+    assert np.array_equal(r1["spectrum"][:den.dim], r0["spectrum"][:den.dim])
+    assert all(np.array_equal(a, b) for a, b in zip(r1["trun"].mats, r0["trun"].mats))
+    rng = np.random.default_rng(7)
+    psi2 = rng.standard_normal(gs.dim) + 1j * rng.standard_normal(gs.dim)
+    den2 = ctx.get_density_matrix(side, [gs.vec, psi2])
+    w2 = type(gs)(gs.sys_len, gs.env_len, gs.secs, psi2)
+    for k, (sub, m) in enumerate(zip(den2.subs, den2.mats)):
+        a, b = gs.sector(k), w2.sector(k)
+        want = (a @ a.conj().T + b @ b.conj().T) / 2 if side == 0 else (a.conj().T @ a + b.conj().T @ b) / 2
+        assert np.max(np.abs(m - want)) <= 1e-12 * max(np.max(np.abs(want)), 1.0)
+
+
+@pytest.mark.gpu
 def test_renormalization_matches_oracle(captured):
     cfg, cap, ctx = captured
     side = 0 if cap["sys_side"] else 1

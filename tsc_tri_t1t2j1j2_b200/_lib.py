@@ -18,11 +18,12 @@ P = ctypes.POINTER
 EXPORTED = [
     "tsc_create", "tsc_destroy", "tsc_last_error", "tsc_tot_num_up", "tsc_superblock_set",
     "tsc_superblock_dim", "tsc_hpsi", "tsc_hpsi_device", "tsc_lanczos", "tsc_truncate",
+    "tsc_density_matrix", "tsc_truncation_operator",
     "tsc_renormalize", "tsc_wave_transform", "tsc_dmrg_run", "tsc_set_capture", "tsc_get_capture",
     "tsc_hpsi_stats", "tsc_stream", "tsc_hpsi_noalloc", "tsc_set_precision", "tsc_set_split_wait_limit",
     "tsc_set_resident_limit", "tsc_spill_stats", "tsc_split_views",
     "tsc_checkpoint_write", "tsc_checkpoint_read", "tsc_set_split_refinement",
-    "tsc_blocksparse_set", "tsc_blocksparse_apply", "tsc_measure_density", "tsc_measure_density_cor", "tsc_measure_correlation",
+    "tsc_blocksparse_set", "tsc_blocksparse_apply", "tsc_measure_density", "tsc_measure_density_cor", "tsc_measure_correlation", "tsc_measure_pair_correlation",
     "tsc_set_autotune",
     "tsc_autotune_table", "tsc_autotune_superblock",
 ]
@@ -37,7 +38,7 @@ class SweepConfig(ctypes.Structure):
     _fields_ = [("kept_min", c_int), ("kept_max_warmup", c_int), ("nsweeps", c_int),
                 ("sweep_kept_max", P(c_int)), ("lanzero", c_double), ("seed", ctypes.c_ulonglong),
                 ("warmup_only", c_int), ("final_half_sweep", c_int), ("resume", c_int), ("max_solves", c_int),
-                ("lanzero_warmup", c_double)]
+                ("lanzero_warmup", c_double), ("final_stop", c_int)]
 
 
 class StepLog(ctypes.Structure):
@@ -80,6 +81,9 @@ def load():
     L.tsc_lanczos.argtypes = [c_void, pd, c_double, pi, pd]
     L.tsc_truncate.argtypes = [c_void, c_int, pd, c_int, c_int, c_double, pi, pd, pd, pd, P(pi), P(c_ll), P(pd),
                                P(c_ll), pd, c_ll]
+    L.tsc_density_matrix.argtypes = [c_void, c_int, pd, c_int, P(pi), P(c_ll), P(pd), P(c_ll)]
+    L.tsc_truncation_operator.argtypes = [c_void, pi, c_ll, pd, c_ll, c_int, c_int, c_double, pi, pd, pd, pd, P(pi),
+                                          P(c_ll), P(pd), P(c_ll), pd, c_ll]
     L.tsc_renormalize.argtypes = [c_void, c_int, c_int, c_int, c_int, pi, c_ll, pd, c_ll, P(pi), P(c_ll), P(pd),
                                   P(c_ll)]
     L.tsc_wave_transform.argtypes = [c_void, c_int, pi, c_ll, pd, c_ll, pd]
@@ -104,6 +108,8 @@ def load():
     L.tsc_measure_density.argtypes = [c_void, ctypes.POINTER(c_double), c_int]
     L.tsc_measure_density_cor.argtypes = [c_void, c_int, ctypes.POINTER(c_double), c_int]
     L.tsc_measure_correlation.argtypes = [c_void, c_int, c_int, ctypes.POINTER(c_double), c_int]
+    L.tsc_measure_pair_correlation.argtypes = [c_void, c_int, c_int, c_int, c_int, ctypes.POINTER(c_int),
+                                               ctypes.POINTER(c_double), c_int]
     L.tsc_set_autotune.argtypes = [c_void, c_int]
     L.tsc_autotune_table.argtypes = [c_void, ctypes.POINTER(c_int), ctypes.POINTER(c_double), c_int]
     L.tsc_autotune_superblock.argtypes = [c_void, c_int]

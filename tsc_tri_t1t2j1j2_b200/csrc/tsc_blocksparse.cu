@@ -162,7 +162,8 @@ void Engine::blocksparse_set(int nprob, const int* ints, long long nints, const 
   bs.p2s.gterms = bs.p2.gterms;
   bs.p1.upload(st);
   bs.p2.upload(st);
-  build_split_views(bs.p1s, bs.p2s, bs.sv, st);
+  // 200 terms share 16 operator sets: one view per operator block, coefficients in the epilogue
+  build_split_views(bs.p1s, bs.p2s, bs.sv, st, true);
   bs.p1s.upload_split(st);
   bs.p2s.upload_split(st);
   bs.p1.gterms.clear();
@@ -174,6 +175,7 @@ void Engine::blocksparse_set(int nprob, const int* ints, long long nints, const 
   bs.nprob = nprob;
   cuda_check(cudaStreamSynchronize(st), "blocksparse sync");
   bs.valid = true;
+  views_of_batch_ = true;
 }
 
 void Engine::blocksparse_apply(const double2* d_in, double2* d_out, bool split) {

@@ -274,6 +274,57 @@ int tsc_truncate(tsc_ctx* ctx, int side, const double* psi, int kept_min, int ke
   });
 }
 
+int tsc_density_matrix(tsc_ctx* ctx, int side, const double* psi, int levels, const int** den_ints,
+                       long long* nden_ints, const double** den_data, long long* nden_cplx) {
+  return guard(ctx, [&] {
+    if (!ctx->eng || !ctx->eng->sb.valid) throw Error(TSC_E_STATE, "no superblock set");
+    if (side != 0 && side != 1) throw Error(TSC_E_ARG, "side must be 0 or 1");
+    if (!psi || levels < 1) throw Error(TSC_E_ARG, "null wave or levels < 1");
+    Engine& E = *ctx->eng;
+    const WLayout& wl = E.sb.wl;
+    const int nw = std::min(levels, 2);   // the reference reads the first two waves
+    DevBuf a((size_t)std::max<long long>(wl.dim * nw, 1), E.st, false);
+    cuda_check(cudaMemcpyAsync(a.p, psi, wl.dim * nw * sizeof(double2), cudaMemcpyHostToDevice, E.st), "h2d");
+    DBlock den = E.density_matrix(side, a.p, wl, levels);
+    ctx->out_ints.clear();
+    ctx->out_data.clear();
+    E.download_block(den, ctx->out_ints, ctx->out_data);
+    if (den_ints) *den_ints = ctx->out_ints.data();
+    if (nden_ints) *nden_ints = (long long)ctx->out_ints.size();
+    if (den_data) *den_data = (const double*)ctx->out_data.data();
+    if (nden_cplx) *nden_cplx = (long long)ctx->out_data.size();
+  });
+}
+
+int tsc_truncation_operator(tsc_ctx* ctx, const int* den_ints, long long nden_ints, const double* den_data,
+                            long long nden_cplx, int kept_min, int kept_max, double trun_err, int* num_state,
+                            double* err, double* entropy, double* entropy_mult, const int** trun_ints,
+                            long long* ntrun_ints, const double** trun_data, long long* ntrun_cplx, double* spectrum,
+                            long long spectrum_cap) {
+  return guard(ctx, [&] {
+    if (!ctx->eng) throw Error(TSC_E_STATE, "no engine");
+    if (!den_ints || !den_data || !num_state) throw Error(TSC_E_ARG, "null buffers");
+    Engine& E = *ctx->eng;
+    Reader r{den_ints, den_ints + nden_ints, (const cplx*)den_data, (const cplx*)den_data + nden_cplx};
+    DBlock den = read_block(E, r);
+    Engine::TruncResult tr;
+    E.truncation_operator(den, kept_min, kept_max, trun_err, tr);
+    *num_state = tr.num_state;
+    if (err) *err = tr.err;
+    if (entropy) *entropy = tr.ent;
+    if (entropy_mult) *entropy_mult = tr.ent_mult;
+    ctx->out_ints.clear();
+    ctx->out_data.clear();
+    E.download_block(tr.trun, ctx->out_ints, ctx->out_data);
+    if (trun_ints) *trun_ints = ctx->out_ints.data();
+    if (ntrun_ints) *ntrun_ints = (long long)ctx->out_ints.size();
+    if (trun_data) *trun_data = (const double*)ctx->out_data.data();
+    if (ntrun_cplx) *ntrun_cplx = (long long)ctx->out_data.size();
+    if (spectrum)
+      for (long long i = 0; i < spectrum_cap && i < (long long)tr.spectrum.size(); ++i) spectrum[i] = tr.spectrum[i];
+  });
+}
+
 int tsc_renormalize(tsc_ctx* ctx, int side, int sys_len, int env_len, int mshift, const int* ints, long long nints,
                     const double* data, long long ncplx, const int** out_ints, long long* nout_ints,
                     const double** out_data, long long* nout_cplx) {
@@ -334,6 +385,7 @@ int tsc_dmrg_run(tsc_ctx* ctx, const tsc_sweep_config* sw, tsc_step_log* log, in
     std::vector<int> sweeps(sw->sweep_kept_max, sw->sweep_kept_max + sw->nsweeps);
     std::vector<Engine::StepRec> recs;
     ctx->eng->lanzero_warmup_ = sw->lanzero_warmup > 0 ? sw->lanzero_warmup : 0.0;
+    ctx->eng->final_stop_ = sw->final_stop > 0 ? sw->final_stop : 0;
     ctx->eng->run(sw->kept_min, sw->kept_max_warmup, sweeps, sw->lanzero, sw->seed, &recs, sw->warmup_only != 0,
                   sw->final_half_sweep != 0, sw->resume != 0, sw->max_solves > 0 ? sw->max_solves : 0);
     nsteps = (int)recs.size();
@@ -379,6 +431,9 @@ int tsc_set_precision(tsc_ctx* ctx, int mode, double split_tol) {
     if (mode != TSC_FP64 && mode != TSC_SPLIT_BF16) throw Error(TSC_E_ARG, "unknown precision mode");
     ctx->eng->precision_ = mode;
     if (split_tol > 0) ctx->eng->split_tol_ = split_tol;
+    // the split form's pre-sliced operand views take about 1.5x the superblock's
+    // FP64 operator and intermediate memory: the stored models get less by default
+    ctx->eng->model_store().set_default_frac(mode == TSC_SPLIT_BF16 ? 0.30 : 0.45);
   });
 }
 
@@ -400,8 +455,10 @@ int tsc_set_split_wait_limit(tsc_ctx* ctx, long long polls) {
 
 int tsc_split_views(tsc_ctx* ctx, long long* bytes, int* views) {
   return guard(ctx, [&] {
-    if (!ctx->eng || !ctx->eng->sb.valid) throw Error(TSC_E_STATE, "no superblock set");
-    const SplitData& sd = ctx->eng->sb.sv;
+    if (!ctx->eng) throw Error(TSC_E_STATE, "no engine");
+    Engine& E = *ctx->eng;
+    if (E.views_of_batch_ ? !E.bs.valid : !E.sb.valid) throw Error(TSC_E_STATE, "no superblock set");
+    const SplitData& sd = E.views_of_batch_ ? E.bs.sv : E.sb.sv;
     for (int a = 0; a < 3; ++a) {
       if (bytes) bytes[a] = sd.units[a] * (long long)SPLIT_UNIT;
       if (views) views[a] = sd.nviews[a];

@@ -279,8 +279,8 @@ DBlock Engine::oper_ndia_in_block(const SiteOp& so, int old_idx, int new_idx, bo
   return trun_ndia(out, it->second);
 }
 
-// Change_sys_oper_ndia / Change_env_oper_ndia (get_sys.f90:1672-1723), Truns = .true.
-DBlock Engine::carry_ndia(const DBlock& op, int from, int to, bool sys, char flag) {
+// Change_sys_oper_ndia / Change_env_oper_ndia (get_sys.f90:1672-1723); Truns = trunc_end
+DBlock Engine::carry_ndia(const DBlock& op, int from, int to, bool sys, char flag, bool trunc_end) {
   const auto& bsm = sys ? sys_bsm : env_bsm;
   const auto& truns = sys ? sys_truns : env_truns;
   const int trun_idx = 1;
@@ -294,27 +294,52 @@ DBlock Engine::carry_ndia(const DBlock& op, int from, int to, bool sys, char fla
   }
   DBlock out = block_ndia(cur, bsm.at(idx + 1), !sys, flag);
   auto it = truns.find(to);
-  if (it == truns.end()) return out;
+  if (!trunc_end || it == truns.end()) return out;
   return trun_ndia(out, it->second);
 }
 
-// block_mul_block_ndia (block.f90:376-635) with Flag1 = Flag2 = 'N', coefficient 1,
-// coupled to total rank 0: product[k] = sum_mid c(k, mid) o1[.., mid] o2[mid, k],
-// the 3j sums of block.f90:584-613 as written
-DBlock Engine::product_to_scalar(const DBlock& o1, const DBlock& o2, const Basis& basis) {
+// block_mul_block_ndia (block.f90:376-635) with Flag1 = Flag2 = 'N', coefficient 1:
+// (o1 o2) coupled to rank K on the sectors of `basis`; sub-block (sector, new
+// spin) exists for new spin in |S-K| .. S+K present in the basis, and
+// product[k] = sum_mid c(k, mid) o1[.., mid] o2[mid, k] with the 3j sums of
+// block.f90:584-613 as written
+DBlock Engine::product_ndia(const DBlock& o1, const DBlock& o2, int K, const Basis& basis) {
+  const int up_dif = o1.up_dif + o2.up_dif, up_dif2 = o2.up_dif, K1 = o1.down_dif, K2 = o2.down_dif;
+  DBlock p;
+  p.len = basis.len;
+  p.up_dif = up_dif;
+  p.down_dif = K;
+  long long off = 0;
+  for (int x = 0; x < basis.num; ++x) {
+    const int nd = basis.sec[x].num_down;
+    for (int nnd = std::abs(nd - K); nnd <= nd + K; nnd += 2) {
+      const int y = basis.find(basis.sec[x].num_up + up_dif, nnd);
+      if (y < 0) continue;
+      SubDesc d;
+      d.num_up = basis.sec[x].num_up;
+      d.num_down = nd;
+      d.down_dif = nnd - nd;
+      d.row_dim = basis.sec[y].dim;
+      d.sdim = basis.sec[x].dim;
+      d.off = off;
+      off += (long long)d.row_dim * d.sdim;
+      p.dim += d.sdim;
+      p.sub.push_back(d);
+    }
+  }
+  p.num = (int)p.sub.size();
+  p.buf = std::make_shared<DevBuf>((size_t)std::max<long long>(off, 1), st, false);
   TaskList tl;
-  std::vector<int> g;
-  DBlock p = ndia_layout(basis, o1.up_dif + o2.up_dif, 0, tl, g);
-  const int up_dif2 = o2.up_dif, K1 = o1.down_dif, K2 = o2.down_dif;
   for (int i = 0; i < p.num; ++i) {
     const SubDesc& s = p.sub[i];
+    const int g = tl.add_group(p.ptr(i), BASE_ABS, 0, s.row_dim, s.row_dim, s.sdim, 0);
     const int num_up = s.num_up, num_down = s.num_down, new_num_down = num_down + s.down_dif;
     for (int mid = std::abs(num_down - K2); mid <= num_down + K2; mid += 2) {
       const int i2 = find_sub3(o2, num_up, num_down, mid - num_down);
       const int i1 = find_sub3(o1, num_up + up_dif2, mid, new_num_down - mid);
       if (i1 < 0 || i2 < 0) continue;
       const int kq = new_num_down - num_down;
-      const double c11 = w3j(new_num_down, 0, num_down, -new_num_down, kq, num_down);
+      const double c11 = w3j(new_num_down, K, num_down, -new_num_down, kq, num_down);
       if (c11 == 0.0) throw Error(TSC_E_QN, "correlation: vanishing 3j normalisation");
       double c1 = 0.0;
       for (int m6 = -mid; m6 <= mid; m6 += 2) {
@@ -322,7 +347,7 @@ DBlock Engine::product_to_scalar(const DBlock& o1, const DBlock& o2, const Basis
         double c12 = w3j(new_num_down, K1, mid, -new_num_down, m5, m6);
         const int m44 = -m6, m55 = -m44 - num_down;
         c12 *= w3j(mid, K2, num_down, m44, m55, num_down) * pm1((mid + m44) / 2);
-        c12 *= w3j(K1, K2, 0, m5, m55, -kq) * pm1((-K1 + K2 + kq) / 2);
+        c12 *= w3j(K1, K2, K, m5, m55, -kq) * pm1((-K1 + K2 + kq) / 2) * std::sqrt(K + 1.0);
         c1 += c12;
       }
       if (c1 == 0.0) continue;
@@ -336,7 +361,7 @@ DBlock Engine::product_to_scalar(const DBlock& o1, const DBlock& o2, const Basis
       t.r_ld = o2.sub[i2].row_dim;
       t.l_op = t.r_op = OP_N;
       t.K = o1.sub[i1].sdim;
-      tl.gterms[g[i]].push_back(t);
+      tl.gterms[g].push_back(t);
     }
   }
   tl.upload(st);
@@ -599,7 +624,7 @@ std::vector<cplx> Engine::measure_oper_cor(const SiteOp& op1, const SiteOp& op2,
   for (int j = xi + ny; j <= sl - 1; j += ny) {
     DBlock a = oper_ndia_in_block(op1, xi, j, true, false, flag);
     DBlock b = oper_ndia_in_block(op2, j, j, true, false, flag);
-    DBlock p = product_to_scalar(a, b, sys_bsm.at(j));
+    DBlock p = product_ndia(a, b, 0, sys_bsm.at(j));
     auto it = sys_truns.find(j);
     DBlock q = (j <= 1 || it == sys_truns.end()) ? p : trun_dia(p, it->second);
     DBlock s = carry_dia(q, j, sl - 1, true);
@@ -639,6 +664,96 @@ std::vector<cplx> Engine::measure_oper_cor(const SiteOp& op1, const SiteOp& op2,
   return out;
 }
 
+// ---- singlet pair correlations (Get_mSCOP_Operator_Cor0, measure.f90:2683-2834) ----
+//
+// O+_ab = (c+_{a up} c+_{b dn} - c+_{a dn} c+_{b up}) / sqrt(2) (measure.f90:5441-5442)
+// is the rank-0 coupling of two st_elec_up, formed at the longer length.
+
+// Get_sys_two (measure.f90:2837-2874): O+_{idx1 idx2} on the system block of
+// length idx2, truncated there
+DBlock Engine::sys_pair(int idx1, int idx2) {
+  DBlock a = oper_ndia_in_block(st_elec_up, idx1, idx2, true, false, 'F');
+  DBlock b = oper_ndia_in_block(st_elec_up, idx2, idx2, true, false, 'F');
+  DBlock p = product_ndia(a, b, 0, sys_bsm.at(idx2));
+  auto it = sys_truns.find(idx2);
+  if (idx2 <= 1 || it == sys_truns.end()) return p;
+  return trun_ndia(p, it->second);
+}
+
+// Get_sys_two1 (measure.f90:2877-2932): the pair of length idx2 times st_elec_down
+// at idx3 (coupled to rank 1/2), times st_elec_down at idx4 (coupled to rank 0),
+// carried into the system block of the wave
+DBlock Engine::sys_pair_four(int idx2, int idx3, int idx4, const DBlock& pair) {
+  const int sl = disk_layout.sys_len;
+  DBlock m = carry_ndia(pair, idx2, idx3, true, 'B', false);
+  DBlock c3 = oper_ndia_in_block(st_elec_down, idx3, idx3, true, false, 'F');
+  DBlock t3 = product_ndia(m, c3, 1, sys_bsm.at(idx3));
+  auto it3 = sys_truns.find(idx3);
+  if (idx3 > 1 && it3 != sys_truns.end()) t3 = trun_ndia(t3, it3->second);
+  DBlock m4 = carry_ndia(t3, idx3, idx4, true, 'F', false);
+  DBlock c4 = oper_ndia_in_block(st_elec_down, idx4, idx4, true, false, 'F');
+  DBlock t4 = product_ndia(m4, c4, 0, sys_bsm.at(idx4));
+  auto it4 = sys_truns.find(idx4);
+  if (idx4 > 1 && it4 != sys_truns.end()) t4 = trun_dia(t4, it4->second);
+  return carry_dia(t4, idx4, sl - 1, true);
+}
+
+// Get_SCOP_Operator_Env, Flags 'S0' (measure.f90:5450-5505): O+_{idx1 idx2} on the
+// environment block of length idx2, carried to new_idx (truncated there when trunc_end)
+DBlock Engine::env_pair(int idx1, int idx2, int new_idx, bool trunc_end) {
+  DBlock a = oper_ndia_in_block(st_elec_up, idx1, idx2, false, false, 'F');
+  DBlock b = oper_ndia_in_block(st_elec_up, idx2, idx2, false, false, 'F');
+  DBlock e = product_ndia(a, b, 0, env_bsm.at(idx2));
+  auto it = env_truns.find(idx2);
+  if (idx2 > 1 && it != env_truns.end()) e = trun_ndia(e, it->second);
+  return carry_ndia(e, idx2, new_idx, false, 'B', trunc_end);
+}
+
+// Get_mSCOP_Operator_Cor0 from label 11 (the part main.f90:259-262 reaches), Flags
+// 'S0': the pair on the bond (xc1, neib(xc1, ij1)) against the bonds (s3, neib(s3,
+// 1|3|5)) for s3 on the leg of xc1 up to xc2, first in the system block, then in
+// the environment block (values conjugated there, as the reference writes them)
+std::vector<Engine::PairCor> Engine::measure_pair_cor(int xc1, int xc2, int ij, int ij1) {
+  if (!disk_wave || disk_layout.num == 0) throw Error(TSC_E_STATE, "no ground state: run tsc_dmrg_run first");
+  const int N = L.num_site, ny = L.Ny, sl = disk_layout.sys_len, el = disk_layout.env_len;
+  if (xc1 < 1 || xc1 > N || ij1 < 1 || ij1 > Lattice::neibt) throw Error(TSC_E_ARG, "pair_cor: bad first bond");
+  if (xc2 > N) throw Error(TSC_E_ARG, "pair_cor: the last site lies past the lattice");
+  std::vector<PairCor> out;
+  const int sid1 = xc1, sid2 = L.NEIB(sid1, ij1);
+  if (sid2 < 1) throw Error(TSC_E_ARG, "pair_cor: the first bond leaves the lattice");
+  const int lo = std::min(sid1, sid2), hi = std::max(sid1, sid2);
+  if (hi > sl - 1) throw Error(TSC_E_ARG, "pair_cor: the first bond must lie in the system block of the wave");
+  const DBlock pair = sys_pair(lo, hi);
+  for (int sid3 = sid1 + ny + ij; sid3 <= sl - 1; sid3 += ny) {
+    if (sid3 <= hi || sid3 > xc2) continue;
+    for (int i = 1; i <= 5; i += 2) {
+      const int sid4 = L.NEIB(sid3, i);
+      if (std::min(sid4, sid3) <= hi) continue;
+      if (std::max(sid3, sid4) > sl - 1) continue;
+      DBlock four = sys_pair_four(hi, std::min(sid3, sid4), std::max(sid3, sid4), pair);
+      double im = 0.0;
+      const double re = expect_dia(&four, nullptr, sys_bsm.at(sl), true, &im);
+      out.push_back(PairCor{sid1, sid2, sid3, sid4, cplx(re, im)});
+    }
+  }
+  const DBlock sys_oper = carry_ndia(pair, hi, sl - 1, true, 'B', true);
+  const int m0 = (sl + 2) % ny, m1 = (sid1 - 1) % ny;
+  for (int sid3 = sl + 2 - m0 + m1 + 1 + ij; sid3 <= xc2; sid3 += ny) {
+    const int eid1 = N - sid3 + 1;
+    if (eid1 > el - 1) continue;
+    for (int i = 1; i <= 5; i += 2) {
+      const int sid4 = L.NEIB(sid3, i);
+      if (sid4 < 1) continue;
+      const int eid2 = N - sid4 + 1;
+      if (std::max(eid1, eid2) > el - 1) continue;
+      DBlock env_oper = env_pair(std::min(eid1, eid2), std::max(eid1, eid2), el - 1, true);
+      const cplx v = corr_env_block_ndia(sys_oper, env_oper, sys_bsm.at(sl), env_bsm.at(el), 'B');
+      out.push_back(PairCor{sid1, sid2, sid3, sid4, std::conj(v)});
+    }
+  }
+  return out;
+}
+
 }  // namespace tsc
 
 using namespace tsc;
@@ -664,6 +779,26 @@ extern "C" int tsc_measure_correlation(tsc_ctx* ctx, int kind, int site, double*
       out[2 * j + 1] = d[j].imag();
     }
     n = (int)d.size();
+  });
+  return rc == TSC_OK ? n : rc;
+}
+
+extern "C" int tsc_measure_pair_correlation(tsc_ctx* ctx, int xc1, int xc2, int ij, int ij1, int* bonds,
+                                            double* values, int cap) {
+  int n = 0;
+  const int rc = guard(ctx, [&] {
+    if (!ctx->eng) throw Error(TSC_E_STATE, "no engine");
+    if (cap > 0 && (!bonds || !values)) throw Error(TSC_E_ARG, "null output");
+    const auto r = ctx->eng->measure_pair_cor(xc1, xc2, ij, ij1);
+    for (int k = 0; k < (int)r.size() && k < cap; ++k) {
+      bonds[4 * k] = r[k].s1;
+      bonds[4 * k + 1] = r[k].s2;
+      bonds[4 * k + 2] = r[k].s3;
+      bonds[4 * k + 3] = r[k].s4;
+      values[2 * k] = r[k].value.real();
+      values[2 * k + 1] = r[k].value.imag();
+    }
+    n = (int)r.size();
   });
   return rc == TSC_OK ? n : rc;
 }

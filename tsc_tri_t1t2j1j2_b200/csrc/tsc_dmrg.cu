@@ -314,62 +314,95 @@ void Engine::lanczos_run(double2* d_psi, double lanzero, double rel_tol, bool sp
 }
 
 // --------------------------------------------------------------- density matrix + truncation
-void Engine::truncate(int side, const double2* d_psi, const WLayout& wl, int kept_min, int kept_max, double trun_err,
-                      TruncResult& out) {
-  const double thr = 1.0000000036274937e-15;   // 1.0E-15 default real, den_mat.f90:278,330
-  // Get_density_matrix_*_new normalises a copy of the wave (den_mat.f90:118-124)
-  DevBuf w((size_t)std::max<long long>(wl.dim, 1), st, false);
-  cuda_check(cudaMemcpyAsync(w.p, d_psi, wl.dim * sizeof(double2), cudaMemcpyDeviceToDevice, st), "copy");
-  normalize(w.p, wl.dim);
-  // rho per sector: sys psi psi^H (den_mat.f90:41-43), env psi^H psi (den_mat.f90:89-91)
-  std::vector<long long> doff(wl.num);
+// Get_density_matrix_sys_new / _env_new (den_mat.f90:103-183): levels = 1 takes
+// the normalised wave, levels >= 2 averages the density matrices of the first two
+// waves, unnormalised, as the reference does (den_mat.f90:127-135); d_psi holds
+// the waves one after the other.  One sub-block per wave sector:
+// sys psi psi^H (den_mat.f90:41-43), env psi^H psi (den_mat.f90:89-91).
+DBlock Engine::density_matrix(int side, const double2* d_psi, const WLayout& wl, int levels) {
+  if (levels < 1) throw Error(-1, "levels must be at least 1");
+  DBlock den;
+  den.len = side == 0 ? wl.sys_len : wl.env_len;
+  den.num = wl.num;
   long long tot = 0;
   for (int k = 0; k < wl.num; ++k) {
-    int d = side == 0 ? wl.sec[k].sys_dim : wl.sec[k].env_dim;
-    doff[k] = tot;
-    tot += (long long)d * d;
+    const WSec& w = wl.sec[k];
+    SubDesc d;
+    d.num_up = side == 0 ? w.sys_num_up : w.env_num_up;
+    d.num_down = side == 0 ? w.sys_num_down : w.env_num_down;
+    d.row_dim = d.sdim = side == 0 ? w.sys_dim : w.env_dim;
+    d.off = tot;
+    tot += (long long)d.sdim * d.sdim;
+    den.dim += d.sdim;
+    den.sub.push_back(d);
   }
-  DevBufP den = std::make_shared<DevBuf>((size_t)std::max<long long>(tot, 1), st, false);
+  den.buf = std::make_shared<DevBuf>((size_t)std::max<long long>(tot, 1), st, false);
+  DevBuf w(levels == 1 ? (size_t)std::max<long long>(wl.dim, 1) : 1, st, false);
+  const double2* src = d_psi;
+  if (levels == 1) {
+    cuda_check(cudaMemcpyAsync(w.p, d_psi, wl.dim * sizeof(double2), cudaMemcpyDeviceToDevice, st), "copy");
+    normalize(w.p, wl.dim);
+    src = w.p;
+  }
   TaskList tl;
   for (int k = 0; k < wl.num; ++k) {
     const WSec& s = wl.sec[k];
-    int d = side == 0 ? s.sys_dim : s.env_dim;
-    int g = tl.add_group(den->p + doff[k], BASE_ABS, 0, d, d, d, 0);
-    GTerm t{};
-    t.kind = TK_GEMM;
-    t.ar = 1.0;
-    t.l_base = t.r_base = BASE_IN;
-    t.l_off = t.r_off = s.off;
-    t.l_ld = t.r_ld = s.sys_dim;
-    if (side == 0) {
-      t.l_op = OP_N;
-      t.r_op = OP_C;
-      t.K = s.env_dim;
-    } else {
-      t.l_op = OP_C;
-      t.r_op = OP_N;
-      t.K = s.sys_dim;
+    const int d = den.sub[k].sdim;
+    const int g = tl.add_group(den.ptr(k), BASE_ABS, 0, d, d, d, 0);
+    for (int l = 0; l < std::min(levels, 2); ++l) {
+      GTerm t{};
+      t.kind = TK_GEMM;
+      t.ar = levels == 1 ? 1.0 : 0.5;
+      t.l_base = t.r_base = BASE_IN;
+      t.l_off = t.r_off = s.off + (long long)l * wl.dim;
+      t.l_ld = t.r_ld = s.sys_dim;
+      if (side == 0) {
+        t.l_op = OP_N;
+        t.r_op = OP_C;
+        t.K = s.env_dim;
+      } else {
+        t.l_op = OP_C;
+        t.r_op = OP_N;
+        t.K = s.sys_dim;
+      }
+      tl.gterms[g].push_back(t);
     }
-    tl.gterms[g].push_back(t);
   }
   tl.upload(st);
-  run_tasks(tl, w.p, nullptr, nullptr);
+  run_tasks(tl, const_cast<double2*>(src), nullptr, nullptr);
+  cuda_check(cudaStreamSynchronize(st), "density matrix sync");
+  return den;
+}
+
+void Engine::truncate(int side, const double2* d_psi, const WLayout& wl, int kept_min, int kept_max, double trun_err,
+                      TruncResult& out) {
+  DBlock den = density_matrix(side, d_psi, wl, 1);
+  truncation_operator(den, kept_min, kept_max, trun_err, out);
+}
+
+// Get_truncation_operator (den_mat.f90:190-418) on a density matrix of one
+// sub-block per sector; den is overwritten by its eigenvectors.
+void Engine::truncation_operator(DBlock& den, int kept_min, int kept_max, double trun_err, TruncResult& out) {
+  const double thr = 1.0000000036274937e-15;   // 1.0E-15 default real, den_mat.f90:278,330
+  const int nsec = den.num;
+  for (const auto& s : den.sub)
+    if (s.row_dim != s.sdim || s.down_dif != 0) throw Error(-1, "density matrix sub-blocks must be square");
   // zheev per sector (den_mat.f90:243): cuSOLVER zheevd, eigenvalues ascending.
   // Sectors are dealt to the lanes largest first, each to the least loaded lane.
   int dim = 0;
-  std::vector<int> eoffs(wl.num);
-  for (int k = 0; k < wl.num; ++k) {
+  std::vector<int> eoffs(nsec);
+  for (int k = 0; k < nsec; ++k) {
     eoffs[k] = dim;
-    dim += side == 0 ? wl.sec[k].sys_dim : wl.sec[k].env_dim;
+    dim += den.sub[k].sdim;
   }
   DevBuf ev((size_t)(dim + 2) / 2 + 1, st, false);
   double* d_ev = reinterpret_cast<double*>(ev.p);
-  DevBuf info((size_t)(wl.num + 1) / 4 + 1, st, true);   // one int per sector
+  DevBuf info((size_t)(nsec + 1) / 4 + 1, st, true);   // one int per sector
   int* d_info = reinterpret_cast<int*>(info.p);
   if (!eig) eig = std::make_shared<EigLanes>(kEigLanes, device_);
-  std::vector<int> order(wl.num);
-  for (int k = 0; k < wl.num; ++k) order[k] = k;
-  auto sdim = [&](int k) { return side == 0 ? wl.sec[k].sys_dim : wl.sec[k].env_dim; };
+  std::vector<int> order(nsec);
+  for (int k = 0; k < nsec; ++k) order[k] = k;
+  auto sdim = [&](int k) { return den.sub[k].sdim; };
   std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return sdim(a) > sdim(b); });
   std::vector<std::vector<int>> mine(kEigLanes);
   std::vector<double> load(kEigLanes, 0.0);
@@ -389,7 +422,7 @@ void Engine::truncate(int side, const double2* d_psi, const WLayout& wl, int kep
     const int maxd = sdim(mine[l].front());
     int lwork = 0;
     if (cusolverDnZheevd_bufferSize(L.h, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, maxd,
-                                    reinterpret_cast<cuDoubleComplex*>(den->p), maxd, d_ev, &lwork) !=
+                                    reinterpret_cast<cuDoubleComplex*>(den.buf->p), maxd, d_ev, &lwork) !=
         CUSOLVER_STATUS_SUCCESS)
       throw Error(-3, "zheevd buffer size");
     if (lwork > L.lwork) {
@@ -399,7 +432,7 @@ void Engine::truncate(int side, const double2* d_psi, const WLayout& wl, int kep
     for (int k : mine[l]) {
       const int d = sdim(k);
       if (cusolverDnZheevd(L.h, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, d,
-                           reinterpret_cast<cuDoubleComplex*>(den->p + doff[k]), d, d_ev + eoffs[k],
+                           reinterpret_cast<cuDoubleComplex*>(den.ptr(k)), d, d_ev + eoffs[k],
                            reinterpret_cast<cuDoubleComplex*>(L.work->p), L.lwork, d_info + k) !=
           CUSOLVER_STATUS_SUCCESS)
         throw Error(-3, "zheevd");
@@ -409,27 +442,27 @@ void Engine::truncate(int side, const double2* d_psi, const WLayout& wl, int kep
   for (int l = 0; l < kEigLanes; ++l)
     if (!mine[l].empty()) cuda_check(cudaStreamWaitEvent(st, eig->lane[l].done, 0), "wait");
   // canonical eigenvector phases (see launch_phase_fix)
-  for (int k = 0; k < wl.num; ++k) {
-    int d = side == 0 ? wl.sec[k].sys_dim : wl.sec[k].env_dim;
-    if (d > 0) cuda_check(launch_phase_fix(den->p + doff[k], d, d, st), "phase_fix");
+  for (int k = 0; k < nsec; ++k) {
+    int d = den.sub[k].sdim;
+    if (d > 0) cuda_check(launch_phase_fix(den.ptr(k), d, d, st), "phase_fix");
   }
   std::vector<double> evh(dim + 1);
   if (dim) cuda_check(cudaMemcpyAsync(evh.data() + 1, d_ev, dim * sizeof(double), cudaMemcpyDeviceToHost, st), "d2h");
-  std::vector<int> infoh(wl.num, 0);
-  if (wl.num) cuda_check(cudaMemcpyAsync(infoh.data(), d_info, wl.num * sizeof(int), cudaMemcpyDeviceToHost, st), "d2h");
+  std::vector<int> infoh(nsec, 0);
+  if (nsec) cuda_check(cudaMemcpyAsync(infoh.data(), d_info, nsec * sizeof(int), cudaMemcpyDeviceToHost, st), "d2h");
   cuda_check(cudaStreamSynchronize(st), "sync");
-  for (int k = 0; k < wl.num; ++k)
+  for (int k = 0; k < nsec; ++k)
     if (infoh[k] != 0) throw Error(-3, "zheevd did not converge");
   // eigenvalues at rounding-noise level count as exact zeros (see null_complete)
   for (int i = 1; i <= dim; ++i)
     if (evh[i] < kZeroWeight) evh[i] = 0.0;
   // den_mat.f90:249-333 on the host (scalars only)
-  std::vector<int> idx(dim + 1), eigs(dim + 1), sidx0(wl.num);
+  std::vector<int> idx(dim + 1), eigs(dim + 1), sidx0(nsec);
   std::vector<double> evs(dim + 1);
   int p = 0;
-  for (int k = 0; k < wl.num; ++k) {
-    int d = side == 0 ? wl.sec[k].sys_dim : wl.sec[k].env_dim;
-    int S2 = side == 0 ? wl.sec[k].sys_num_down : wl.sec[k].env_num_down;
+  for (int k = 0; k < nsec; ++k) {
+    int d = den.sub[k].sdim;
+    int S2 = den.sub[k].num_down;
     sidx0[k] = p + 1;
     for (int i = 0; i < d; ++i) {
       ++p;
@@ -464,7 +497,7 @@ void Engine::truncate(int side, const double2* d_psi, const WLayout& wl, int kep
   double ent = 0.0;
   for (int i = 1; i <= dim; ++i)
     if (evs[i] >= thr) ent = ent - evs[i] * std::log(evs[i]);
-  std::vector<int> cnt(wl.num, 0);
+  std::vector<int> cnt(nsec, 0);
   for (int k = 1; k <= ns; ++k) {
     int id = idx[k];
     int sec = (int)(std::upper_bound(sidx0.begin(), sidx0.end(), id) - sidx0.begin()) - 1;
@@ -474,32 +507,32 @@ void Engine::truncate(int side, const double2* d_psi, const WLayout& wl, int kep
   DBlock& U = out.trun;
   U = DBlock();
   long long uo = 0;
-  for (int k = 0; k < wl.num; ++k) {
+  for (int k = 0; k < nsec; ++k) {
     if (cnt[k] <= 0) continue;
     SubDesc s;
-    s.num_up = side == 0 ? wl.sec[k].sys_num_up : wl.sec[k].env_num_up;
-    s.num_down = side == 0 ? wl.sec[k].sys_num_down : wl.sec[k].env_num_down;
-    s.row_dim = side == 0 ? wl.sec[k].sys_dim : wl.sec[k].env_dim;
+    s.num_up = den.sub[k].num_up;
+    s.num_down = den.sub[k].num_down;
+    s.row_dim = den.sub[k].sdim;
     s.sdim = cnt[k];
     s.off = uo;
     uo += (long long)s.row_dim * s.sdim;
     U.sub.push_back(s);
   }
   U.num = (int)U.sub.size();
-  U.len = side == 0 ? wl.sys_len : wl.env_len;
+  U.len = den.len;
   U.buf = std::make_shared<DevBuf>((size_t)std::max<long long>(uo, 1), st, false);
   // kept columns of every sector; kept zero-weight columns are then replaced by
   // the canonical complement basis on the GPU (null_complete)
   std::vector<NullJob> nulls;
   int ui = 0;
-  for (int k = 0; k < wl.num; ++k) {
+  for (int k = 0; k < nsec; ++k) {
     if (cnt[k] <= 0) continue;
     const SubDesc& s = U.sub[ui++];
     int row = s.row_dim, col = s.sdim;
     int sig = 0;
     for (int c = 0; c < col; ++c)
       if (evh[sidx0[k] + row - col + c] > 0.0) sig++;
-    cuda_check(cudaMemcpyAsync(U.buf->p + s.off, den->p + doff[k] + (long long)(row - col) * row,
+    cuda_check(cudaMemcpyAsync(U.buf->p + s.off, den.ptr(k) + (long long)(row - col) * row,
                                (size_t)row * col * sizeof(double2), cudaMemcpyDeviceToDevice, st),
                "U copy");
     if (sig < col) nulls.push_back(NullJob{U.buf->p + s.off, row, sig, col - sig});
@@ -1503,7 +1536,8 @@ void Engine::run(int kept_min, int kept_warm, const std::vector<int>& sweeps, do
     right_to_left(N - 2, 1, trun_err, log);
   }
   // main.f90:205-206: a last half sweep stops at 5 Num_site / 6, where Measurement reads the wave
-  if (final_half) left_to_right(1, 5 * N / 6 - 1, sweeps.empty() ? tmp_err : trun_err, log);
+  if (final_half)
+    left_to_right(1, final_stop_ > 0 ? final_stop_ : 5 * N / 6 - 1, sweeps.empty() ? tmp_err : trun_err, log);
 }
 
 }  // namespace tsc

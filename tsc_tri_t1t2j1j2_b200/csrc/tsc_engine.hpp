@@ -163,6 +163,7 @@ struct TaskList {
   double exec_flops = 0;   // flops the kernel executes
   long long nterms = 0;
   SplitArenas arenas{};    // split lists: the arenas of their pre-sliced operand views
+  bool term_alpha = false; // split lists: coefficients applied per term by the kernel (not folded)
   int add_group(double2* abs_c, uint8_t base, long long c_off, int ld, int M, int N, int beta);
   // Packs the lists for the device.  Groups whose term list is much longer than
   // total_cost / (slots * waves) are split into contiguous term chunks, each
@@ -190,8 +191,10 @@ class ModelStore {
   }
   void clear() { map_.clear(); resident_ = 0; }
   void bind(cudaStream_t st) { st_ = st; }
-  // bytes of device memory the stored models may hold; < 0: 45 % of the device
+  // bytes of device memory the stored models may hold; < 0: default_frac of the device
   void set_limit(long long bytes) { limit_ = bytes; }
+  // the default's share of device memory (the split form's operand views need room)
+  void set_default_frac(double f) { default_frac_ = f; }
   long long limit() const;
   long long resident_bytes() const { return resident_; }
   long long spills = 0, restores = 0;
@@ -212,6 +215,7 @@ class ModelStore {
   std::map<long long, Entry> map_;
   cudaStream_t st_ = nullptr;
   long long limit_ = -1;
+  double default_frac_ = 0.45;
   long long resident_ = 0;
   unsigned long long clock_ = 0;
 };
@@ -232,7 +236,9 @@ struct SplitData {
 // operand (with the term's coefficient folded in), each rectangle of the input
 // vector, each phase-1 intermediate read by phase 2.  Allocates the arenas,
 // slices the operator views, and keeps the input vector's tile list.
-void build_split_views(TaskList& p1, TaskList& p2, SplitData& sd, cudaStream_t st);
+// term_alpha: keep the terms' coefficients in the lists (applied per term by the
+// kernel's epilogue) instead of folding them into per-term operator views
+void build_split_views(TaskList& p1, TaskList& p2, SplitData& sd, cudaStream_t st, bool term_alpha = false);
 // Slices the input vector's views of sd (before phase 1 of every call).
 void slice_input(const SplitData& sd, const double2* d_in, cudaStream_t st);
 
@@ -293,6 +299,7 @@ class Engine {
     bool valid = false;
   } bs;
   void blocksparse_set(int nprob, const int* ints, long long nints, const cplx* data, long long ncplx);
+  bool views_of_batch_ = false;   // the last set was a block-sparse batch (tsc_split_views reports its views)
   void blocksparse_apply(const double2* d_in, double2* d_out, bool split);
 
   // measurement of the last ground state (csrc/tsc_measure.cu, measure.f90)
@@ -316,14 +323,23 @@ class Engine {
   DBlock block_ndia(const DBlock& blk, const Basis& basis, bool env, char flag);
   DBlock trun_ndia(const DBlock& ori, const DBlock& trun);
   DBlock oper_ndia_in_block(const SiteOp& so, int old_idx, int new_idx, bool sys, bool trunc, char flag);
-  DBlock carry_ndia(const DBlock& op, int from, int to, bool sys, char flag);
-  DBlock product_to_scalar(const DBlock& o1, const DBlock& o2, const Basis& basis);
+  DBlock carry_ndia(const DBlock& op, int from, int to, bool sys, char flag, bool trunc_end = true);
+  DBlock product_ndia(const DBlock& o1, const DBlock& o2, int K, const Basis& basis);
   DBlock transfer_trans(const DBlock& in);
   struct PairSum;
   cplx pair_sum(PairSum& ps);
   cplx corr_site_ndia(const DBlock& bl, const SiteOp& st_op, const Basis& bs, char flag);
   cplx corr_env_site_ndia(const DBlock& bl, const SiteOp& est, const Basis& sbs, const Basis& ebs, char flag);
   cplx corr_env_block_ndia(const DBlock& bl, const DBlock& ebl, const Basis& sbs, const Basis& ebs, char flag);
+  // singlet pair correlations (Get_mSCOP_Operator_Cor0, tsc_correlate.cu)
+  struct PairCor {
+    int s1, s2, s3, s4;
+    cplx value;
+  };
+  std::vector<PairCor> measure_pair_cor(int xc1, int xc2, int ij, int ij1);
+  DBlock sys_pair(int idx1, int idx2);
+  DBlock sys_pair_four(int idx2, int idx3, int idx4, const DBlock& pair);
+  DBlock env_pair(int idx1, int idx2, int new_idx, bool trunc_end);
   // 0: complex FP64 throughout; 1: H.psi sector GEMMs as BF16 slices on the
   // tensor cores, Lanczos finished by FP64 iterations.  Applies from the next
   // superblock set on.
@@ -371,6 +387,8 @@ class Engine {
   };
   void truncate(int side, const double2* d_psi, const WLayout& wl, int kept_min, int kept_max,
                 double trun_err, TruncResult& out);
+  DBlock density_matrix(int side, const double2* d_psi, const WLayout& wl, int levels);
+  void truncation_operator(DBlock& den, int kept_min, int kept_max, double trun_err, TruncResult& out);
   // Kept zero-weight columns of one sector of U: W is the sector's d x (m + sig)
   // block (ld d), m completion columns followed by the sig significant kept
   // eigenvectors; the first m columns are overwritten by the canonical
@@ -415,6 +433,7 @@ class Engine {
   // a run stops once it has made max_solves_ Lanczos solves (0: no cap)
   int max_solves_ = 0;
   double lanzero_warmup_ = 0.0;   // > 0: the warm-up's Lanczos tolerance (else the run's)
+  int final_stop_ = 0;            // > 0: last label of the final half sweep (else 5 N / 6 - 1)
   bool solve_cap_reached() const { return max_solves_ > 0 && nsolve_ >= max_solves_; }
   // the reference's checkpoint files (tsc_checkpoint.cu): every stored model,
   // truncation and basis of the last run and its last wavefunction

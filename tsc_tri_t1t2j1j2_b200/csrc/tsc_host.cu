@@ -566,7 +566,7 @@ int view_tiles_along(const SView& v) {   // row tiles (A) or column tiles (B)
 long long view_units(const SView& v) { return (long long)view_tiles_along(v) * v.nks * (v.role == 0 ? 2 : 1); }
 }  // namespace
 
-void build_split_views(TaskList& p1, TaskList& p2, SplitData& sd, cudaStream_t st) {
+void build_split_views(TaskList& p1, TaskList& p2, SplitData& sd, cudaStream_t st, bool term_alpha) {
   sd = SplitData();
   std::vector<SView> views[3];
   std::map<ViewKey, int> index[3];
@@ -620,10 +620,12 @@ void build_split_views(TaskList& p1, TaskList& p2, SplitData& sd, cudaStream_t s
       const GGroup& g = tl->groups[gi];
       for (GTerm& t : tl->gterms[gi]) {
         if (t.kind != TK_GEMM || t.K <= 0) continue;
-        // the coefficient rides on the operator operand (on A when both are operators)
+        // the coefficient rides on the operator operand (on A when both are
+        // operators), or stays with the term (term_alpha)
         const bool fold_a = t.l_base == BASE_ABS;
-        const double aar = fold_a ? t.ar : 1.0, aai = fold_a ? t.ai : 0.0;
-        const double bar = fold_a ? 1.0 : t.ar, bai = fold_a ? 0.0 : t.ai;
+        const double cr = term_alpha ? 1.0 : t.ar, ci = term_alpha ? 0.0 : t.ai;
+        const double aar = fold_a ? cr : 1.0, aai = fold_a ? ci : 0.0;
+        const double bar = fold_a ? 1.0 : cr, bai = fold_a ? 0.0 : ci;
         auto A = operand(t.l_base, t.l_off, t.l_ld, t.l_op, 0, g.M, t.K, aar, aai);
         auto B = operand(t.r_base, t.r_off, t.r_ld, t.r_op, 1, t.K, g.N, bar, bai);
         const SView& va = views[A.first][A.second];
@@ -635,8 +637,10 @@ void build_split_views(TaskList& p1, TaskList& p2, SplitData& sd, cudaStream_t s
         t.r_off = vb.dst;
         t.r_ld = vb.nks;
         t.l_op = t.r_op = OP_N;
-        t.ar = 1.0;
-        t.ai = 0.0;
+        if (!term_alpha) {
+          t.ar = 1.0;
+          t.ai = 0.0;
+        }
         t.pad0 = 1;   // references pre-sliced views
       }
     }
@@ -683,6 +687,7 @@ void build_split_views(TaskList& p1, TaskList& p2, SplitData& sd, cudaStream_t s
   pack(views[ARENA_IN], tin, sd.in_lists, sd.d_in_views, sd.d_in_tiles);
   sd.n_in_tiles = (int)tin.size();
   p1.arenas = p2.arenas = sd.arenas;
+  p1.term_alpha = p2.term_alpha = term_alpha;
 }
 
 void slice_input(const SplitData& sd, const double2* d_in, cudaStream_t st) {
@@ -808,7 +813,7 @@ void Engine::run_tasks(TaskList& tl, double2* in, double2* out, double2* scr) {
   b.part = tl.part ? tl.part->p : nullptr;
   if (tl.split)
     cuda_check(launch_grouped_zgemm_split(tl.d_jobs, tl.njobs, tl.d_groups, tl.d_terms, b, tl.arenas, d_fault,
-                                          split_wait_limit_, st),
+                                          split_wait_limit_, tl.term_alpha ? 1 : 0, st),
                "grouped_zgemm_split");
   else
     cuda_check(launch_grouped_zgemm(tl.d_jobs, tl.njobs, tl.d_groups, tl.d_terms, b, st, tl.tile), "grouped_zgemm");
@@ -884,7 +889,7 @@ long long ModelStore::limit() const {
     cudaGetLastError();
     return 1ll << 62;
   }
-  return (long long)(0.45 * (double)tot);
+  return (long long)(default_frac_ * (double)tot);
 }
 
 void ModelStore::spill(Entry& e) {

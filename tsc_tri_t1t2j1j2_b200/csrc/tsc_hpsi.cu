@@ -1106,6 +1106,7 @@ void Engine::superblock_set(DModel&& sys, DModel&& env, Basis&& sys_bs, Basis&& 
   build_hpsi_tasks();
   cuda_check(cudaStreamSynchronize(st), "superblock sync");
   sb.valid = true;
+  views_of_batch_ = false;
 }
 
 void Engine::hpsi(const double2* d_in, double2* d_out) { hpsi_form(d_in, d_out, sb.p1s.split); }

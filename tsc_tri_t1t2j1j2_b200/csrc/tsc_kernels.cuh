@@ -98,10 +98,14 @@ cudaError_t launch_slice_tiles(const SView* views, const STile* tiles, int ntile
 // l_off / r_off = the view's first tile (units), l_ld / r_ld = its tiles along K.
 // Every mbarrier wait of the kernel gives up after wait_limit polls; it then
 // sets *fault (the caller's device status word) to 1 and the CTA returns with
-// its tiles partly written.
+// its tiles partly written.  term_alpha = 0: the GEMM terms' coefficients are
+// folded into their operand views (ar = 1, ai = 0 in the list) and accumulator
+// segments run across terms; 1: segments break at every term and the epilogue
+// multiplies each by its term's coefficient (views shared by all terms of an
+// operator).
 cudaError_t launch_grouped_zgemm_split(const GJob* jobs, int njobs, const GGroup* groups, const GTerm* terms,
                                        Bases bases, SplitArenas arenas, int* fault, long long wait_limit,
-                                       cudaStream_t st);
+                                       int term_alpha, cudaStream_t st);
 // default poll limit of the split kernel's waits (far above any wait of a healthy launch)
 constexpr long long SPLIT_WAIT_LIMIT = 1ll << 20;
 constexpr int SPLIT_TILE_M = 128, SPLIT_TILE_N = 64;

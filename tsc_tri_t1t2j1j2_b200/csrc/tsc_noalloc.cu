@@ -85,7 +85,7 @@ extern "C" int tsc_hpsi_noalloc(tsc_ctx* ctx, const void* d_in, void* d_out) {
     for (TaskList* tl : {&a, &b}) {
       if (split)
         cuda_check(launch_grouped_zgemm_split(tl->d_jobs, tl->njobs, tl->d_groups, tl->d_terms, bs, tl->arenas,
-                                              E.d_fault, E.split_wait_limit_, E.st),
+                                              E.d_fault, E.split_wait_limit_, tl->term_alpha ? 1 : 0, E.st),
                    "grouped_zgemm_split");
       else
         cuda_check(launch_grouped_zgemm(tl->d_jobs, tl->njobs, tl->d_groups, tl->d_terms, bs, E.st, tl->tile),

@@ -17,7 +17,9 @@
 // are done in FP64.
 //
 // Operands arrive pre-sliced.  Every GEMM operand is a view -- an operator
-// block (with the term's coefficient folded in, sliced once per superblock), a
+// block (with the term's coefficient folded in, sliced once per superblock; or,
+// with term_alpha, shared by all terms of that operator, the epilogue then
+// scaling each term's own segments by its coefficient), a
 // rectangle of the input vector (sliced once per call by slice_tiles_kernel),
 // or a phase-1 intermediate (sliced by the phase-1 launch's own epilogue) --
 // stored as stage tiles: six BF16 planes in the canonical K-major, no-swizzle
@@ -254,14 +256,26 @@ __device__ __forceinline__ int job_steps(const GJob& job, const GTerm* terms) {
   return n;
 }
 
-// Persistent, warp-specialised: warps 0..11 produce stages (one chunk per
-// thread per step, the next step's loads in flight while the current one is
-// converted), warp 12 issues the MMAs (one elected lane) into one of two TMEM
-// accumulators, warps 13..16 drain the other accumulator into the outputs.
+// number of accumulator segments of a job: SP_SEG steps each over the job's
+// steps in order, or, with term_alpha, over each GEMM term's steps alone (a
+// segment then belongs to one term and the epilogue applies its coefficient)
+__device__ __forceinline__ int job_segments(const GJob& job, const GTerm* terms, int term_alpha) {
+  if (!term_alpha) return (job_steps(job, terms) + SP_SEG - 1) / SP_SEG;
+  int n = 0;
+  for (int ti = job.t0; ti < job.t1; ++ti) {
+    const GTerm t = terms[ti];
+    if (t.kind == TK_GEMM && t.K > 0) n += ((t.K + SP_TK - 1) / SP_TK + SP_SEG - 1) / SP_SEG;
+  }
+  return n;
+}
+
+// Persistent, warp-specialised (roles as described at the top of the file):
+// warp 0 streams the stages, warp 1 issues the MMAs into one of two TMEM
+// accumulators, warps 2..9 drain the other accumulator into the outputs.
 __global__ void __launch_bounds__(SP_THREADS, 1)
 grouped_zgemm_split_kernel(const GJob* __restrict__ jobs, int njobs, const GGroup* __restrict__ groups,
                            const GTerm* __restrict__ terms, Bases bases, SplitArenas arenas, int* fault,
-                           long long wait_limit) {
+                           long long wait_limit, int term_alpha) {
   extern __shared__ __align__(1024) unsigned char smem[];
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + SP_STAGES * STAGE_BYTES);
   uint64_t* empty = full + SP_STAGES;
@@ -358,41 +372,49 @@ grouped_zgemm_split_kernel(const GJob* __restrict__ jobs, int njobs, const GGrou
       int q = 0, sg = 0;   // stage use, accumulator segment (over the CTA's jobs)
       bool ok = true;
       for (int jb = blockIdx.x; jb < njobs && ok; jb += gridDim.x) {
-        const int nst = job_steps(jobs[jb], terms);
-        for (int i = 0; i < nst; ++i, ++q) {
-          const int si = i % SP_SEG;
-          const int a = sg & 1, ua = sg >> 1;
-          if (si == 0) {   // a segment starts: wait until the epilogue has drained this accumulator
-            if (ua >= 1 && !mbar_wait(smem_u32(&acce[a]), (uint32_t)((ua - 1) & 1), abort_flag, wait_limit)) {
+        const GJob job = jobs[jb];
+        const int nst = job_steps(job, terms);
+        int i = 0, si = 0;   // step of the job, step within the current segment
+        for (int ti = job.t0; ti < job.t1 && ok; ++ti) {
+          const GTerm t = terms[ti];
+          if (t.kind != TK_GEMM || t.K <= 0) continue;
+          const int nk = (t.K + SP_TK - 1) / SP_TK;
+          for (int kk = 0; kk < nk; ++kk, ++i, ++q) {
+            const int a = sg & 1, ua = sg >> 1;
+            if (si == 0) {   // a segment starts: wait until the epilogue has drained this accumulator
+              if (ua >= 1 && !mbar_wait(smem_u32(&acce[a]), (uint32_t)((ua - 1) & 1), abort_flag, wait_limit)) {
+                ok = false;
+                break;
+              }
+              fence_after_sync();
+            }
+            const uint32_t dhr = tmem + a * (4 * SP_TN), dhi = dhr + SP_TN, dlr = dhr + 2 * SP_TN, dli = dhr + 3 * SP_TN;
+            const int s = q % SP_STAGES;
+            if (!mbar_wait(smem_u32(&full[s]), (uint32_t)((q / SP_STAGES) & 1), abort_flag, wait_limit)) {
               ok = false;
               break;
             }
             fence_after_sync();
-          }
-          const uint32_t dhr = tmem + a * (4 * SP_TN), dhi = dhr + SP_TN, dlr = dhr + 2 * SP_TN, dli = dhr + 3 * SP_TN;
-          const int s = q % SP_STAGES;
-          if (!mbar_wait(smem_u32(&full[s]), (uint32_t)((q / SP_STAGES) & 1), abort_flag, wait_limit)) {
-            ok = false;
-            break;
-          }
-          fence_after_sync();
-          const uint32_t a0 = smem_u32(smem + s * STAGE_BYTES), b0 = a0 + 6 * A_PLANE;
+            const uint32_t a0 = smem_u32(smem + s * STAGE_BYTES), b0 = a0 + 6 * A_PLANE;
 #pragma unroll
-          for (int pi = 0; pi < 6; ++pi) {
-            const int sa = c_pairs[pi][0], sb = c_pairs[pi][1];
-            const uint64_t ar = smem_desc(a0 + (2 * sa) * A_PLANE), ai = smem_desc(a0 + (2 * sa + 1) * A_PLANE);
-            const uint64_t br = smem_desc(b0 + (2 * sb) * B_PLANE), bi = smem_desc(b0 + (2 * sb + 1) * B_PLANE);
-            const uint32_t dcr = pi == 0 ? dhr : dlr, dci = pi == 0 ? dhi : dli;
-            const uint32_t first = (si == 0 && pi <= 1) ? 0u : 1u;   // first write of hi (pi 0) and lo (pi 1)
-            umma_bf16(dcr, ar, br, IDESC, first);          // Cr  = Ar Br
-            umma_bf16(dcr, ai, bi, IDESC_NEG_A, 1u);       // Cr -= Ai Bi
-            umma_bf16(dci, ar, bi, IDESC, first);          // Ci  = Ar Bi
-            umma_bf16(dci, ai, br, IDESC, 1u);             // Ci += Ai Br
-          }
-          umma_commit(smem_u32(&empty[s]));
-          if (si == SP_SEG - 1 || i == nst - 1) {   // segment complete: hand it to the epilogue
-            umma_commit(smem_u32(&accf[a]));
-            sg++;
+            for (int pi = 0; pi < 6; ++pi) {
+              const int sa = c_pairs[pi][0], sb = c_pairs[pi][1];
+              const uint64_t ar = smem_desc(a0 + (2 * sa) * A_PLANE), ai = smem_desc(a0 + (2 * sa + 1) * A_PLANE);
+              const uint64_t br = smem_desc(b0 + (2 * sb) * B_PLANE), bi = smem_desc(b0 + (2 * sb + 1) * B_PLANE);
+              const uint32_t dcr = pi == 0 ? dhr : dlr, dci = pi == 0 ? dhi : dli;
+              const uint32_t first = (si == 0 && pi <= 1) ? 0u : 1u;   // first write of hi (pi 0) and lo (pi 1)
+              umma_bf16(dcr, ar, br, IDESC, first);          // Cr  = Ar Br
+              umma_bf16(dcr, ai, bi, IDESC_NEG_A, 1u);       // Cr -= Ai Bi
+              umma_bf16(dci, ar, bi, IDESC, first);          // Ci  = Ar Bi
+              umma_bf16(dci, ai, br, IDESC, 1u);             // Ci += Ai Br
+            }
+            umma_commit(smem_u32(&empty[s]));
+            ++si;
+            if (si == SP_SEG || i == nst - 1 || (term_alpha && kk == nk - 1)) {   // segment complete: to the epilogue
+              umma_commit(smem_u32(&accf[a]));
+              sg++;
+              si = 0;
+            }
           }
         }
       }
@@ -411,8 +433,7 @@ grouped_zgemm_split_kernel(const GJob* __restrict__ jobs, int njobs, const GGrou
     for (int jb = blockIdx.x; jb < njobs && ok; jb += gridDim.x) {
       const GJob job = jobs[jb];
       const GGroup g = groups[job.group];
-      const int nst = job_steps(job, terms);
-      const int nseg = (nst + SP_SEG - 1) / SP_SEG;
+      const int nseg = job_segments(job, terms, term_alpha);
       const int m0 = job.tm * SP_TM, n0 = job.tn * SP_TN;
       const int row = m0 + quad * 32 + lane;
       const bool partial = job.part >= 0;
@@ -422,10 +443,23 @@ grouped_zgemm_split_kernel(const GJob* __restrict__ jobs, int njobs, const GGrou
       const bool slice_out = !partial && g.s_off >= 0;
       const int s_nks = (g.N + SP_TK - 1) / SP_TK;
       const int npass = nseg > 0 ? nseg : 1;
+      int ecur = job.t0, erem = 0;         // term_alpha: the segment's term and its steps not yet covered
+      double alr = 1.0, ali = 0.0;         // ... and its coefficient
       // one pass per accumulator segment (one pass of zeros for a job of element terms only);
       // the first writes beta * C_old + element terms + segment, later ones add to what it wrote
       for (int sgi = 0; sgi < npass; ++sgi) {
         const int a = sg & 1, ua = sg >> 1;
+        if (term_alpha && nseg > 0) {
+          while (erem == 0 && ecur < job.t1) {
+            const GTerm t = terms[ecur++];
+            if (t.kind == TK_GEMM && t.K > 0) {
+              erem = (t.K + SP_TK - 1) / SP_TK;
+              alr = t.ar;
+              ali = t.ai;
+            }
+          }
+          erem -= erem < SP_SEG ? erem : SP_SEG;
+        }
         if (nseg > 0) {
           // warp-uniform: the tensor-memory loads below need every lane
           if (!__all_sync(0xffffffffu, mbar_wait(smem_u32(&accf[a]), (uint32_t)(ua & 1), abort_flag, wait_limit))) {
@@ -449,8 +483,9 @@ grouped_zgemm_split_kernel(const GJob* __restrict__ jobs, int njobs, const GGrou
             tmem_ld8(lane_base + 3 * SP_TN + c0, li);
 #pragma unroll
             for (int j = 0; j < 8; ++j) {
-              cr[j] = (double)hr[j] + (double)lr[j];
-              ci[j] = (double)hi[j] + (double)li[j];
+              const double sr = (double)hr[j] + (double)lr[j], si = (double)hi[j] + (double)li[j];
+              cr[j] = alr * sr - ali * si;
+              ci[j] = alr * si + ali * sr;
             }
           } else {
 #pragma unroll
@@ -542,7 +577,7 @@ grouped_zgemm_split_kernel(const GJob* __restrict__ jobs, int njobs, const GGrou
 
 cudaError_t launch_grouped_zgemm_split(const GJob* jobs, int njobs, const GGroup* groups, const GTerm* terms,
                                        Bases bases, SplitArenas arenas, int* fault, long long wait_limit,
-                                       cudaStream_t st) {
+                                       int term_alpha, cudaStream_t st) {
   if (njobs <= 0) return cudaSuccess;
   if (!fault || wait_limit < 0) return cudaErrorInvalidValue;
   static std::atomic<unsigned long long> attr{0};
@@ -554,7 +589,7 @@ cudaError_t launch_grouped_zgemm_split(const GJob* jobs, int njobs, const GGroup
   if (nsm <= 0) nsm = 148;
   const int grid = njobs < nsm ? njobs : nsm;
   grouped_zgemm_split_kernel<<<grid, SP_THREADS, SMEM_BYTES, st>>>(jobs, njobs, groups, terms, bases, arenas,
-                                                                    fault, wait_limit);
+                                                                    fault, wait_limit, term_alpha ? 1 : 0);
   return cudaGetLastError();
 }
 

@@ -226,6 +226,42 @@ class Context:
         return {"trun": trun, "num_state": ns.value, "err": err.value, "entropy": ent.value,
                 "entropy_mult": entm.value, "spectrum": spec}
 
+    def get_density_matrix(self, side, waves, levels=None):
+        """Get_density_matrix_sys_new (side 0, den_mat.f90:103-138) / _env_new (side 1,
+        den_mat.f90:143-177) on the current superblock: `waves` is one vector or a
+        list of vectors (levels of them; the reference averages the first two when
+        levels >= 2).  Returns the density matrix as a Block."""
+        ws = [waves] if np.ndim(waves) == 1 else list(waves)
+        levels = len(ws) if levels is None else int(levels)
+        x = np.ascontiguousarray(np.concatenate([np.asarray(w, np.complex128) for w in ws[:2]]))
+        ti, tn, td, tc = P(ctypes.c_int)(), ctypes.c_longlong(), P(ctypes.c_double)(), ctypes.c_longlong()
+        self._check(self.L.tsc_density_matrix(self.h, side, _dptr(x), levels, ctypes.byref(ti), ctypes.byref(tn),
+                                              ctypes.byref(td), ctypes.byref(tc)))
+        ints = np.ctypeslib.as_array(ti, shape=(tn.value,)).copy()
+        data = (np.ctypeslib.as_array(td, shape=(2 * tc.value,)).copy().view(np.complex128)
+                if tc.value else np.zeros(0, np.complex128))
+        return Block.read(Cursor(ints, data))
+
+    def truncation_from_density(self, den: Block, kept_min, kept_max, trun_err):
+        """Get_truncation_operator (den_mat.f90:190-418) on a given density matrix."""
+        ints, data = [], []
+        den.write(ints, data)
+        ints, data = pack(ints, data)
+        ns = ctypes.c_int()
+        err, ent, entm = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        ti, tn, td, tc = P(ctypes.c_int)(), ctypes.c_longlong(), P(ctypes.c_double)(), ctypes.c_longlong()
+        spec = np.zeros(max(1, int(den.dim)), np.float64)
+        self._check(self.L.tsc_truncation_operator(self.h, _iptr(ints), len(ints), _dptr(data), len(data), kept_min,
+                                                   kept_max, trun_err, ctypes.byref(ns), ctypes.byref(err),
+                                                   ctypes.byref(ent), ctypes.byref(entm), ctypes.byref(ti),
+                                                   ctypes.byref(tn), ctypes.byref(td), ctypes.byref(tc), _dptr(spec),
+                                                   len(spec)))
+        ints = np.ctypeslib.as_array(ti, shape=(tn.value,)).copy()
+        data = (np.ctypeslib.as_array(td, shape=(2 * tc.value,)).copy().view(np.complex128)
+                if tc.value else np.zeros(0, np.complex128))
+        return {"trun": Block.read(Cursor(ints, data)), "num_state": ns.value, "err": err.value,
+                "entropy": ent.value, "entropy_mult": entm.value, "spectrum": spec}
+
     def get_hamiltonian(self, side, model: Model, basis: Basis, trun: Block, sys_len, env_len, mshift=0):
         """Get_Hamiltonian_Sys (side 0) / Get_Hamiltonian_Env (side 1): enlarge + renormalise."""
         ints, data = [], []
@@ -261,16 +297,17 @@ class Context:
     # ------------------------------------------------------------------ full run
     def get_ground_state(self, kept_min, kept_warm, sweeps, lanzero=-1.0, seed=1, capture_step=-1, max_steps=100000,
                          warmup_only=False, final_half_sweep=False, resume=False, max_solves=0,
-                         lanzero_warmup=-1.0):
+                         lanzero_warmup=-1.0, final_stop=0):
         """Get_Ground_State (main.f90:114-209); resume=True continues with the sweeps
         from the state checkpoint_read loaded (no warm-up, no first half sweeps);
         max_solves > 0 stops the run after that many DMRG steps; lanzero_warmup > 0
-        sets the warm-up's tolerance alone."""
+        sets the warm-up's tolerance alone; final_stop > 0 ends the final half
+        sweep at that label instead of 5 Num_site / 6 - 1."""
         self._check(self.L.tsc_set_capture(self.h, capture_step))
         sk = (ctypes.c_int * max(1, len(sweeps)))(*sweeps)
         cfg = _lib.SweepConfig(kept_min, kept_warm, len(sweeps), sk, lanzero, seed, 1 if warmup_only else 0,
                                1 if final_half_sweep else 0, 1 if resume else 0, int(max_solves),
-                               float(lanzero_warmup))
+                               float(lanzero_warmup), int(final_stop))
         logs = (_lib.StepLog * max_steps)()
         n = self._check(self.L.tsc_dmrg_run(self.h, ctypes.byref(cfg), logs, max_steps))
         out = []
@@ -316,6 +353,28 @@ class Context:
         self._check(self.L.tsc_measure_correlation(self.h, self.COR_KINDS[kind], int(site),
                                                    out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), n))
         return out[0::2] + 1j * out[1::2]
+
+    def measure_pair_correlation(self, xc1, xc2=None, ij=0, ij1=1):
+        """Singlet pair correlations (Get_mSCOP_Operator_Cor0, Flags 'S0',
+        measure.f90:2683-2834; main.f90:259-262 calls it with xc1 = xi1, xc2 =
+        xj1, ij = 0, ij1 = 1 | 3 | 5): [(s1, s2, s3, s4, value)] for the bond
+        (xc1, neib(xc1, ij1)) against the bonds (s3, neib(s3, 1|3|5)) the
+        reference visits; xc2 defaults to the reference's xj1 = 3 Nx / 4 Ny + 2,
+        capped at the lattice."""
+        if xc2 is None:
+            xc2 = min(self.Nx * 3 // 4 * self.Ny + 2, self.Nx * self.Ny)
+        cap = 256
+        while True:
+            bonds = np.zeros(4 * cap, dtype=np.int32)
+            vals = np.zeros(2 * cap, dtype=np.float64)
+            n = self._check(self.L.tsc_measure_pair_correlation(
+                self.h, int(xc1), int(xc2), int(ij), int(ij1), bonds.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                vals.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), cap))
+            if n <= cap:
+                break
+            cap = n
+        return [(int(bonds[4 * k]), int(bonds[4 * k + 1]), int(bonds[4 * k + 2]), int(bonds[4 * k + 3]),
+                 complex(vals[2 * k], vals[2 * k + 1])) for k in range(n)]
 
     def capture(self):
         ti, tn, td, tc = P(ctypes.c_int)(), ctypes.c_longlong(), P(ctypes.c_double)(), ctypes.c_longlong()
