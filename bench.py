@@ -446,25 +446,36 @@ def config1_leg(dev, with_cpu):
     return res
 
 
-def config5_leg(torch, dev, zgemm_peak):
+def config5_leg(torch, dev, zgemm_peak, ks=(64,), batch=True):
     """The benchmark list's synthetic block-sparse H.psi (tsc_blocksparse_*): one
-    problem of K=64 sectors, dimensions log-uniform in [16, 2048], 8 left and 8
-    right operator sets with sector shifts in -2..2, 200 terms with alpha ~ U[-1,1];
-    and a batch of 32 independent problems of uneven size (K in 16..64, dimensions
-    in [16, 256]) applied in one pair of launches.  FP64 and split forms, the
-    split form's largest absolute deviation from the FP64 result."""
+    problem of K sectors per K in `ks` (the list names 64, 128, 256, 400),
+    dimensions log-uniform in [16, 2048], 8 left and 8 right operator sets with
+    sector shifts in -2..2, 200 terms with alpha ~ U[-1,1]; and a batch of 32
+    independent problems of uneven size (K in 16..64, dimensions in [16, 256])
+    applied in one pair of launches.  FP64 and split forms, the split form's
+    largest absolute deviation from the FP64 result."""
     from tsc_tri_t1t2j1j2_b200 import Context
-    from tsc_tri_t1t2j1j2_b200.blocksparse import random_psi, synthetic
+    from tsc_tri_t1t2j1j2_b200.blocksparse import pack, random_psi, synthetic, synthetic_packed
     out = {"workload": "synthetic block-sparse H.psi: entries re/im N(0,1), shift-0 blocks Hermitian; "
-                       "single: K=64 dims log-uniform [16,2048] 8+8 sets 200 terms; "
+                       "single (K=64; K<n> for other K): dims log-uniform [16,2048] 8+8 sets 200 terms; "
                        "batch32: 32 problems K in 16..64 dims [16,256] 8+8 sets 200 terms each, one launch pair"}
     rng = np.random.default_rng(SEED + 5)
-    cases = {"single": [synthetic(rng, 64, 16, 2048)],
-             "batch32": [synthetic(rng, int(k), 16, 256) for k in rng.integers(16, 65, 32)]}
-    for name, probs in cases.items():
+
+    def single(k):   # K = 64 keeps the generator state of the default leg
+        r = rng if k == 64 else np.random.default_rng(SEED + 5 + k)
+        P, ints, data = synthetic_packed(r, k, 16, 2048)
+        return [P], (1, ints, data), r
+
+    cases = [("single" if k == 64 else f"K{k}", lambda k=k: single(k)) for k in ks]
+    if batch:
+        cases.append(("batch32", lambda: (lambda pr: (pr, pack(pr), rng))(
+            [synthetic(rng, int(k), 16, 256) for k in rng.integers(16, 65, 32)])))
+    for name, make in cases:
+        probs, packed, prng = make()
         ctx = Context(device=dev.index, **MODEL)
-        n, flops, xflops = ctx.blocksparse_set(probs)
-        x = torch.from_numpy(random_psi(rng, probs)).to(dev)
+        n, flops, xflops = ctx.blocksparse_set_packed(*packed)
+        del packed
+        x = torch.from_numpy(random_psi(prng, probs)).to(dev)
         ys = {}
         res = {"problems": len(probs), "psi_amplitudes": n, "gflop_per_application": flops / 1e9,
                "gflop_executed": xflops / 1e9}
@@ -490,6 +501,7 @@ def config5_leg(torch, dev, zgemm_peak):
         res["split_max_abs_err"] = float(np.max(np.abs(ys["split"] - ys["fp64"])))
         res["split_max_rel_err"] = res["split_max_abs_err"] / float(np.max(np.abs(ys["fp64"])))
         res["split_speedup"] = res["fp64"]["ms"] / res["split"]["ms"]
+        res["split_operator_view_bytes"] = ctx.split_views()["operators"][0]
         out[name] = res
         ctx.close()
     return out
@@ -718,20 +730,25 @@ def dmrg_steps(args):
 
 
 def sweep_study(args):
-    """The YC4x12 whole run of the sweep leg four ways: FP64 at lanzero 1e-13 (the
+    """The YC4x12 whole run of the sweep leg five ways: FP64 at lanzero 1e-13 (the
     converged reference energy), the split form with the reference's stop for its
-    FP64 finish, the split form with the residual stop 0.1 sqrt(lanzero), and
-    FP64 at lanzero 1e-10.  Prints one JSON line: seconds, iterations and each
-    final energy's distance from the FP64 and the converged runs."""
+    FP64 finish, the split form with the residual stop 0.1 sqrt(lanzero), the
+    split form with its U^H O U renormalisation split too, and FP64 at lanzero
+    1e-10.  Prints one JSON line: seconds, iterations and each final energy's
+    distance from the FP64 and the converged runs."""
     from tsc_tri_t1t2j1j2_b200 import Context
-    runs = (("fp64_lanzero_1e-13", Context.FP64, 1e-13, None), ("split_reference_stop", Context.SPLIT_BF16, 1e-10, 0.0),
-            ("split_residual_0.1", Context.SPLIT_BF16, 1e-10, 0.1), ("fp64", Context.FP64, 1e-10, None))
+    runs = (("fp64_lanzero_1e-13", Context.FP64, 1e-13, None, False),
+            ("split_reference_stop", Context.SPLIT_BF16, 1e-10, 0.0, False),
+            ("split_residual_0.1", Context.SPLIT_BF16, 1e-10, 0.1, False),
+            ("split_renormalization_split", Context.SPLIT_BF16, 1e-10, 0.0, True),
+            ("fp64", Context.FP64, 1e-10, None, False))
     out = {"workload": SWEEP_WORKLOAD}
-    for name, mode, lz, refine in runs:
+    for name, mode, lz, refine, renorm in runs:
         ctx = Context(device=0, **MODEL)
         ctx.set_precision(mode, 1e-11)
         if refine is not None:
             ctx.set_split_refinement(refine)
+        ctx.set_split_renormalization(renorm)
         t0 = time.perf_counter()
         st = ctx.get_ground_state(**dict(SWEEP_CONFIG, lanzero=lz))
         wall = time.perf_counter() - t0
@@ -740,7 +757,8 @@ def sweep_study(args):
         out[name] = {"wall_seconds": wall, "sweep_seconds": sum(x["step_seconds"] for x in sw),
                      "lanczos_seconds": sum(x["lanczos_seconds"] for x in sw),
                      "lanczos_iters": int(sum(x["lanczos_iters"] for x in sw)),
-                     "split_iters": int(sum(x["split_iters"] for x in sw)), "final_e0": st[-1]["e0"]}
+                     "split_iters": int(sum(x["split_iters"] for x in sw)), "final_e0": st[-1]["e0"],
+                     "grow_seconds": sum(x["grow_seconds"] for x in sw)}
     t, f = out["fp64_lanzero_1e-13"]["final_e0"], out["fp64"]["final_e0"]
     for name, *_ in runs:
         e = out[name]["final_e0"]
@@ -768,9 +786,17 @@ def main():
     ap.add_argument("--dmrg-steps", type=int, default=0,
                     help="instead of the bench line: config-3 warm-up + this many m=4000 DMRG steps in both forms")
     ap.add_argument("--dmrg-forms", default="fp64,split", help="forms run by --dmrg-steps (comma-separated)")
+    ap.add_argument("--config5", default="",
+                    help="instead of the bench line: the synthetic block-sparse H.psi for these K (comma-separated)")
     args = ap.parse_args()
     if args.dmrg_steps > 0:
         return dmrg_steps(args)
+    if args.config5:
+        import torch
+        dev = torch.device("cuda", 0)
+        ks = tuple(int(k) for k in args.config5.split(","))
+        print(json.dumps(config5_leg(torch, dev, fp64_peak_tflops(torch, dev), ks, batch=False)), flush=True)
+        return 0
     if args.sweep_study:
         return sweep_study(args)
     if args.warmup < 3:

@@ -311,6 +311,14 @@ int tsc_set_split_refinement(tsc_ctx* ctx, double residual_factor);
  * All zero in the FP64 form. */
 int tsc_split_views(tsc_ctx* ctx, long long* bytes, int* views);
 
+/* Split form only: on = 1 runs the U^H O U renormalisation of block growth
+ * (update_trun_dia / update_trun_ndia, block.f90:3465-3683, inside
+ * tsc_renormalize and tsc_dmrg_run after the warm-up) on the split kernel too,
+ * as eff = (U_l^H O) U_r; 0 (the default) keeps it FP64.  Its ~1e-7 relative
+ * error stays in every later Hamiltonian, where no FP64 Lanczos refinement can
+ * remove it. */
+int tsc_set_split_renormalization(tsc_ctx* ctx, int on);
+
 /* Poll limit of every bounded mbarrier wait in the split-precision kernel (no
  * counterpart in the reference; default 1<<20, far above any wait of a healthy
  * launch).  A wait that runs out sets the context's status word and the kernel

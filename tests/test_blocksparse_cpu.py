@@ -42,3 +42,15 @@ def test_synthetic_rules():
                 assert np.allclose(b, b.conj().T)
     x = random_psi(rng, [P])
     assert len(x) == P.psi_len() and abs(np.linalg.norm(x) - 1) < 1e-12
+
+
+def test_synthetic_packed_equals_pack_of_synthetic():
+    """The packed generator (used for the K = 128..400 synthetic problems) draws
+    the same numbers in the same order as synthetic() + pack()."""
+    import numpy as np
+    from tsc_tri_t1t2j1j2_b200.blocksparse import pack, synthetic, synthetic_packed
+    for K in (1, 4, 11):
+        n, ints, data = pack([synthetic(np.random.default_rng(K), K, 3, 50)])
+        P, ints2, data2 = synthetic_packed(np.random.default_rng(K), K, 3, 50)
+        assert n == 1 and np.array_equal(ints, ints2) and np.array_equal(data, data2)
+        assert P.K == K and len(P.terms) == 200

@@ -157,3 +157,30 @@ def test_split_wait_timeout_is_reported_and_context_recovers(captured):
     ctx.hpsi_device(x.data_ptr(), y.data_ptr())
     torch.cuda.synchronize()
     assert rel(y.cpu().numpy(), cap["hpsi"].vec) <= 2e-5
+
+
+@pytest.mark.gpu
+def test_split_renormalization_error(captured):
+    """tsc_set_split_renormalization: Get_Hamiltonian_Sys/Env with U^H O U on the
+    split kernel, against the same growth in FP64 (the oracle's renormalised
+    model to 1e-12).  Every renormalised block within 2e-6 of the largest
+    element of H, and not bit-equal (the split path ran); this error would stay
+    in every later Hamiltonian, hence the FP64 default."""
+    cap, ctx = captured
+    side = 0 if cap["sys_side"] else 1
+    pre = cap["sys"] if side == 0 else cap["env"]
+    sys_len, env_len = cap["sys"].len, cap["env"].len
+    mshift = 0 if side == 0 else (sys_len + 1)
+    ctx.set_split_renormalization(True)
+    try:
+        grown = ctx.get_hamiltonian(side, pre, cap["grow_basis"], cap["trun"], sys_len, env_len, mshift)
+    finally:
+        ctx.set_split_renormalization(False)
+    ref = cap["grown"]
+    scale = max(np.max(np.abs(m)) for m in ref.ham.mats)
+    err = max(np.max(np.abs(a - b), initial=0.0) for a, b in zip(grown.ham.mats, ref.ham.mats))
+    for oa, ob in zip(grown.ops, ref.ops):
+        for ba, bb in zip(oa, ob):
+            for a, b in zip(ba.mats, bb.mats):
+                err = max(err, float(np.max(np.abs(a - b), initial=0.0)))
+    assert 0.0 < err <= 2e-6 * scale

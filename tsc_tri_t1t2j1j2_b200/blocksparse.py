@@ -89,6 +89,50 @@ def synthetic(rng, K, dmin, dmax, n_left=8, n_right=8, n_terms=200, shifts=(-2, 
     return P
 
 
+def synthetic_packed(rng, K, dmin, dmax, n_left=8, n_right=8, n_terms=200, shifts=(-2, -1, 0, 1, 2)):
+    """synthetic() for one problem written straight into pack()'s layout: the same
+    random draws in the same order, so (1, ints, data) equals
+    pack([synthetic(rng, ...)]) for the same generator state, without holding
+    the blocks twice (K = 400 operator sets take ~45 GB).  Returns (Problem with
+    dims, shifts and terms but no blocks, ints, data)."""
+    d = np.exp(rng.uniform(np.log(dmin), np.log(dmax), K)).astype(int).tolist()
+    e = np.exp(rng.uniform(np.log(dmin), np.log(dmax), K)).astype(int).tolist()
+    P = Problem(d=d, e=e)
+    ls = [int(rng.choice(shifts)) for _ in range(n_left)]
+    rs = [ls[k % n_left] for k in range(n_right)]
+    sizes = [dims[i + s_] * dims[i] for s_, dims in [(s_, d) for s_ in ls] + [(s_, e) for s_ in rs]
+             for i in range(K) if 0 <= i + s_ < K]
+    data = np.empty(int(sum(sizes)) + n_terms, np.complex128)
+    pos = 0
+    for s_, dims in [(s_, d) for s_ in ls] + [(s_, e) for s_ in rs]:
+        for i in range(K):
+            j = i + s_
+            if not 0 <= j < K:
+                continue
+            b = rng.standard_normal((dims[j], dims[i])) + 1j * rng.standard_normal((dims[j], dims[i]))
+            if s_ == 0:
+                b = 0.5 * (b + b.conj().T)
+            data[pos:pos + b.size] = b.ravel(order="F")
+            pos += b.size
+    P.left = [(s_, None) for s_ in ls]
+    P.right = [(s_, None) for s_ in rs]
+    by_shift = {}
+    for bi, s_ in enumerate(rs):
+        by_shift.setdefault(s_, []).append(bi)
+    for _ in range(n_terms):
+        a = int(rng.integers(n_left))
+        bb = int(rng.choice(by_shift[ls[a]]))
+        P.terms.append((complex(rng.uniform(-1.0, 1.0)), a, bb))
+    data[pos:] = [t[0] for t in P.terms]
+    ints = [K, n_left, n_right, n_terms]
+    for x, y in zip(d, e):
+        ints += [int(x), int(y)]
+    ints += ls + rs
+    for _, a, bb in P.terms:
+        ints += [a, bb]
+    return P, np.asarray(ints, np.int32), data
+
+
 def random_psi(rng, problems):
     n = sum(P.psi_len() for P in problems)
     x = rng.standard_normal(n) + 1j * rng.standard_normal(n)

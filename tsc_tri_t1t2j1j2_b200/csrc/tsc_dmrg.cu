@@ -930,6 +930,11 @@ void Engine::grow(int side, DModel& pre, const Basis& basis, const DBlock& trun,
   res.sub.resize(L.num_site + 1);
   TaskList t1, t2;
   long long mid_elems = 0;
+  // optional split form of the renormalisation: eff = (U_l^H O) U_r, so that the
+  // phase-1 intermediate is the A operand of phase 2 as the split kernel wants
+  const bool split_uou = split_renorm_ && precision_ == 1 && !in_warmup_;
+  TaskList s1, s2;
+  long long mid2_elems = 0;
   struct Job {
     const DBlock* ori;
     DBlock* eff;
@@ -1022,6 +1027,37 @@ void Engine::grow(int side, DModel& pre, const Basis& basis, const DBlock& trun,
       b.r_op = OP_N;
       b.K = orow;
       t2.gterms[g2].push_back(b);
+      if (split_uou) {
+        const long long m2 = mid2_elems;
+        mid2_elems += (long long)ldim * ocol;
+        const int h1 = s1.add_group(nullptr, BASE_SCR, m2, ldim, ldim, ocol, 0);
+        GTerm c{};   // U_l^H O
+        c.kind = TK_GEMM;
+        c.ar = 1.0;
+        c.l_base = c.r_base = BASE_ABS;
+        c.l_off = absoff(trun.ptr(lid));
+        c.l_ld = trun.sub[lid].row_dim;
+        c.l_op = OP_C;
+        c.r_off = absoff(ori.ptr(oid));
+        c.r_ld = orow;
+        c.r_op = OP_N;
+        c.K = orow;
+        s1.gterms[h1].push_back(c);
+        const int h2 = s2.add_group(eff.ptr(i), BASE_ABS, 0, ldim, ldim, rd, 0);
+        GTerm d{};   // (U_l^H O) U_r
+        d.kind = TK_GEMM;
+        d.ar = 1.0;
+        d.l_base = BASE_SCR;
+        d.l_off = m2;
+        d.l_ld = ldim;
+        d.l_op = OP_N;
+        d.r_base = BASE_ABS;
+        d.r_off = absoff(trun.ptr(rid));
+        d.r_ld = trun.sub[rid].row_dim;
+        d.r_op = OP_N;
+        d.K = ocol;
+        s2.gterms[h2].push_back(d);
+      }
     }
   };
   for (int ii = 1; ii <= L.nleg11[N1]; ++ii)
@@ -1030,12 +1066,24 @@ void Engine::grow(int side, DModel& pre, const Basis& basis, const DBlock& trun,
       plan(next.sub[ii].op[o], res.sub[ii].op[o]);
     }
   plan(next.ham, res.ham);
-  DevBuf mid((size_t)std::max<long long>(mid_elems, 1), st, false);
-  t1.upload(st);
-  t2.upload(st);
-  run_tasks(t1, nullptr, nullptr, mid.p);
-  run_tasks(t2, nullptr, nullptr, mid.p);
-  cuda_check(cudaStreamSynchronize(st), "grow sync");
+  if (split_uou) {
+    SplitData sv;
+    build_split_views(s1, s2, sv, st);
+    s1.upload_split(st);
+    s2.upload_split(st);
+    DevBuf mid2((size_t)std::max<long long>(mid2_elems, 1), st, false);
+    run_tasks(s1, nullptr, nullptr, mid2.p);
+    run_tasks(s2, nullptr, nullptr, mid2.p);
+    cuda_check(cudaStreamSynchronize(st), "grow sync");
+    check_split_fault();
+  } else {
+    DevBuf mid((size_t)std::max<long long>(mid_elems, 1), st, false);
+    t1.upload(st);
+    t2.upload(st);
+    run_tasks(t1, nullptr, nullptr, mid.p);
+    run_tasks(t2, nullptr, nullptr, mid.p);
+    cuda_check(cudaStreamSynchronize(st), "grow sync");
+  }
   pre = std::move(res);
 }
 

@@ -350,6 +350,9 @@ class Engine {
   // (successive Ritz values within lanzero, eigen.f90:101)
   double refine_res_ = 0.0;
   bool split_now_ = false;    // the current superblock's solve uses the split form
+  // split form only: the U^H O U renormalisation of block growth on the split
+  // kernel too (off by default: its ~1e-7 relative error stays in every later H)
+  bool split_renorm_ = false;
   bool in_warmup_ = false;    // set while the warm-up (infinite-lattice) steps run
 
   // Autotuner of the FP64 H.psi schedule: for each size class (log2 of the

@@ -136,6 +136,14 @@ __device__ __forceinline__ void tmem_ld8(uint32_t taddr, float* v) {
   for (int i = 0; i < 8; ++i) v[i] = __uint_as_float(r[i]);
 }
 
+// the same load without its wait: several in flight, then one tmem_wait_ld()
+__device__ __forceinline__ void tmem_ld8_nowait(uint32_t taddr, uint32_t* r) {
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+               : "r"(taddr));
+}
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
 __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
   uint32_t r[16];
   asm volatile(
@@ -426,8 +434,9 @@ grouped_zgemm_split_kernel(const GJob* __restrict__ jobs, int njobs, const GGrou
     __syncwarp();
   } else {
     // ---------------------------------------------------------------- epilogue
+    constexpr int NCB = SP_TN / 16;          // 8-column chunks of one epilogue warp
     const int quad = warp & 3;               // TMEM lane quadrant this warp may read
-    const int cb0 = ((warp - 2) >> 2) * (SP_TN / 16);   // its half of the tile's 8-column chunks
+    const int cb0 = ((warp - 2) >> 2) * NCB; // its half of the tile's 8-column chunks
     int sg = 0;
     bool ok = true;
     for (int jb = blockIdx.x; jb < njobs && ok; jb += gridDim.x) {
@@ -442,14 +451,18 @@ grouped_zgemm_split_kernel(const GJob* __restrict__ jobs, int njobs, const GGrou
       const bool acc_old = !partial && g.beta;
       const bool slice_out = !partial && g.s_off >= 0;
       const int s_nks = (g.N + SP_TK - 1) / SP_TK;
-      const int npass = nseg > 0 ? nseg : 1;
       int ecur = job.t0, erem = 0;         // term_alpha: the segment's term and its steps not yet covered
       double alr = 1.0, ali = 0.0;         // ... and its coefficient
-      // one pass per accumulator segment (one pass of zeros for a job of element terms only);
-      // the first writes beta * C_old + element terms + segment, later ones add to what it wrote
-      for (int sgi = 0; sgi < npass; ++sgi) {
+      // the job's segments summed in FP64 registers (this lane's row, the warp's 32 columns);
+      // the output tile is then written once
+      double accr[NCB][8], acci[NCB][8];
+#pragma unroll
+      for (int c = 0; c < NCB; ++c)
+#pragma unroll
+        for (int j = 0; j < 8; ++j) accr[c][j] = acci[c][j] = 0.0;
+      for (int sgi = 0; sgi < nseg; ++sgi) {
         const int a = sg & 1, ua = sg >> 1;
-        if (term_alpha && nseg > 0) {
+        if (term_alpha) {
           while (erem == 0 && ecur < job.t1) {
             const GTerm t = terms[ecur++];
             if (t.kind == TK_GEMM && t.K > 0) {
@@ -460,108 +473,105 @@ grouped_zgemm_split_kernel(const GJob* __restrict__ jobs, int njobs, const GGrou
           }
           erem -= erem < SP_SEG ? erem : SP_SEG;
         }
-        if (nseg > 0) {
-          // warp-uniform: the tensor-memory loads below need every lane
-          if (!__all_sync(0xffffffffu, mbar_wait(smem_u32(&accf[a]), (uint32_t)(ua & 1), abort_flag, wait_limit))) {
-            fail();
-            ok = false;
-            break;
-          }
-          fence_after_sync();
+        // warp-uniform: the tensor-memory loads below need every lane
+        if (!__all_sync(0xffffffffu, mbar_wait(smem_u32(&accf[a]), (uint32_t)(ua & 1), abort_flag, wait_limit))) {
+          fail();
+          ok = false;
+          break;
         }
+        fence_after_sync();
         const uint32_t lane_base = tmem + a * (4 * SP_TN) + ((uint32_t)(quad * 32) << 16);
-#pragma unroll 1
-        for (int cb = cb0; cb < cb0 + SP_TN / 16; ++cb) {
-          const int c0 = cb * 8;
-          double cr[8], ci[8];
-          __syncwarp();
-          if (nseg > 0) {
-            float hr[8], hi[8], lr[8], li[8];
-            tmem_ld8(lane_base + c0, hr);
-            tmem_ld8(lane_base + SP_TN + c0, hi);
-            tmem_ld8(lane_base + 2 * SP_TN + c0, lr);
-            tmem_ld8(lane_base + 3 * SP_TN + c0, li);
 #pragma unroll
-            for (int j = 0; j < 8; ++j) {
-              const double sr = (double)hr[j] + (double)lr[j], si = (double)hi[j] + (double)li[j];
-              cr[j] = alr * sr - ali * si;
-              ci[j] = alr * si + ali * sr;
+        for (int c = 0; c < NCB; ++c) {
+          const int c0 = (cb0 + c) * 8;
+          uint32_t hr[8], hi[8], lr[8], li[8];
+          tmem_ld8_nowait(lane_base + c0, hr);
+          tmem_ld8_nowait(lane_base + SP_TN + c0, hi);
+          tmem_ld8_nowait(lane_base + 2 * SP_TN + c0, lr);
+          tmem_ld8_nowait(lane_base + 3 * SP_TN + c0, li);
+          tmem_wait_ld();
+#pragma unroll
+          for (int j = 0; j < 8; ++j) {
+            const double sr = (double)__uint_as_float(hr[j]) + (double)__uint_as_float(lr[j]);
+            const double si = (double)__uint_as_float(hi[j]) + (double)__uint_as_float(li[j]);
+            accr[c][j] += alr * sr - ali * si;
+            acci[c][j] += alr * si + ali * sr;
+          }
+        }
+        // this warp's part of the accumulator is read out: hand it back to the MMA warp
+        fence_before_sync();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(smem_u32(&acce[a]));
+        sg++;
+      }
+      if (!ok) break;
+      // element terms (AXPY / DIAG) in FP64, as grouped_zgemm applies them
+      for (int ti = job.t0; ti < job.t1; ++ti) {
+        const GTerm t = terms[ti];
+        if (t.kind == TK_GEMM) continue;
+        const double2* R = bases.p[t.r_base] + t.r_off;
+        const int rr = row - t.r0;
+        if (row >= g.M || rr < 0 || rr >= t.rm) continue;
+#pragma unroll
+        for (int c = 0; c < NCB; ++c)
+#pragma unroll
+          for (int j = 0; j < 8; ++j) {
+            const int col = n0 + (cb0 + c) * 8 + j, cc = col - t.c0;
+            if (col >= g.N || cc < 0 || cc >= t.rn) continue;
+            double xr, xi;
+            if (t.kind == TK_AXPY) {
+              const double2 x = (t.r_op == OP_N) ? R[(long long)rr + (long long)cc * t.r_ld]
+                                                 : R[(long long)cc + (long long)rr * t.r_ld];
+              xr = x.x;
+              xi = (t.r_op == OP_C) ? -x.y : x.y;
+            } else {
+              if (rr != cc) continue;
+              xr = 1.0;
+              xi = 0.0;
             }
-          } else {
+            accr[c][j] += t.ar * xr - t.ai * xi;
+            acci[c][j] += t.ar * xi + t.ai * xr;
+          }
+      }
 #pragma unroll
-            for (int j = 0; j < 8; ++j) cr[j] = ci[j] = 0.0;
-          }
-          if (nseg > 0 && cb == cb0 + SP_TN / 16 - 1) {   // its part of the accumulator read out: hand it back
-            fence_before_sync();
-            __syncwarp();
-            if (lane == 0) mbar_arrive(smem_u32(&acce[a]));
-          }
-          if (sgi == 0) {
-            // element terms (AXPY / DIAG) in FP64, as grouped_zgemm applies them
-            for (int ti = job.t0; ti < job.t1; ++ti) {
-              const GTerm t = terms[ti];
-              if (t.kind == TK_GEMM) continue;
-              const double2* R = bases.p[t.r_base] + t.r_off;
-              const int rr = row - t.r0;
-              if (row >= g.M || rr < 0 || rr >= t.rm) continue;
-#pragma unroll
-              for (int j = 0; j < 8; ++j) {
-                const int col = n0 + c0 + j, cc = col - t.c0;
-                if (col >= g.N || cc < 0 || cc >= t.rn) continue;
-                double xr, xi;
-                if (t.kind == TK_AXPY) {
-                  const double2 x = (t.r_op == OP_N) ? R[(long long)rr + (long long)cc * t.r_ld]
-                                                     : R[(long long)cc + (long long)rr * t.r_ld];
-                  xr = x.x;
-                  xi = (t.r_op == OP_C) ? -x.y : x.y;
-                } else {
-                  if (rr != cc) continue;
-                  xr = 1.0;
-                  xi = 0.0;
-                }
-                cr[j] += t.ar * xr - t.ai * xi;
-                ci[j] += t.ar * xi + t.ai * xr;
-              }
-            }
-          }
-          if (row < g.M) {
+      for (int c = 0; c < NCB; ++c) {
+        const int c0 = (cb0 + c) * 8;
+        if (row < g.M) {
+          if (acc_old) {
             // all eight old values in flight before any store (the stores could alias them)
-            if (sgi > 0 || acc_old) {
-              double2 o[8];
-#pragma unroll
-              for (int j = 0; j < 8; ++j) {
-                const int col = n0 + c0 + j;
-                o[j] = col < g.N ? C[(long long)row + (long long)col * ldc] : make_double2(0.0, 0.0);
-              }
-#pragma unroll
-              for (int j = 0; j < 8; ++j) {
-                cr[j] += o[j].x;
-                ci[j] += o[j].y;
-              }
-            }
+            double2 o[8];
 #pragma unroll
             for (int j = 0; j < 8; ++j) {
               const int col = n0 + c0 + j;
-              if (col < g.N) C[(long long)row + (long long)col * ldc] = make_double2(cr[j], ci[j]);
+              o[j] = col < g.N ? C[(long long)row + (long long)col * ldc] : make_double2(0.0, 0.0);
             }
-            // a phase-1 intermediate read by the next launch as an A operand: its final
-            // values also go, sliced, into the A tiles of its view (rows >= M and columns
-            // >= N of those tiles stay zero from the arena's initial clearing).  Column
-            // chunks past the view's last k-step belong to no tile of this row: writing
-            // them would land in the next row tile's tiles.
-            if (slice_out && sgi == npass - 1 && (n0 + c0) / SP_TK < s_nks) {
-              double2 v[8];
 #pragma unroll
-              for (int j = 0; j < 8; ++j)
-                v[j] = (n0 + c0 + j) < g.N ? make_double2(cr[j], ci[j]) : make_double2(0.0, 0.0);
-              const int col0 = n0 + c0;
-              const long long unit = g.s_off + 2ll * ((long long)job.tm * s_nks + col0 / SP_TK);
-              if (unit + 2 <= arenas.units[ARENA_T])
-                store_chunk(arenas.a[ARENA_T] + unit * SPLIT_UNIT, A_PLANE, chunk_off(row - m0, (col0 / 8) & 1), v);
+            for (int j = 0; j < 8; ++j) {
+              accr[c][j] += o[j].x;
+              acci[c][j] += o[j].y;
             }
           }
+#pragma unroll
+          for (int j = 0; j < 8; ++j) {
+            const int col = n0 + c0 + j;
+            if (col < g.N) C[(long long)row + (long long)col * ldc] = make_double2(accr[c][j], acci[c][j]);
+          }
+          // a phase-1 intermediate read by the next launch as an A operand: its final
+          // values also go, sliced, into the A tiles of its view (rows >= M and columns
+          // >= N of those tiles stay zero from the arena's initial clearing).  Column
+          // chunks past the view's last k-step belong to no tile of this row: writing
+          // them would land in the next row tile's tiles.
+          if (slice_out && (n0 + c0) / SP_TK < s_nks) {
+            double2 v[8];
+#pragma unroll
+            for (int j = 0; j < 8; ++j)
+              v[j] = (n0 + c0 + j) < g.N ? make_double2(accr[c][j], acci[c][j]) : make_double2(0.0, 0.0);
+            const int col0 = n0 + c0;
+            const long long unit = g.s_off + 2ll * ((long long)job.tm * s_nks + col0 / SP_TK);
+            if (unit + 2 <= arenas.units[ARENA_T])
+              store_chunk(arenas.a[ARENA_T] + unit * SPLIT_UNIT, A_PLANE, chunk_off(row - m0, (col0 / 8) & 1), v);
+          }
         }
-        if (nseg > 0) sg++;
       }
     }
   }

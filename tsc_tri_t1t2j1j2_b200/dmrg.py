@@ -118,6 +118,11 @@ class Context:
         lanzero, eigen.f90:101)."""
         self._check(self.L.tsc_set_split_refinement(self.h, float(residual_factor)))
 
+    def set_split_renormalization(self, on: bool):
+        """Split form only: U^H O U of block growth on the split kernel too (off by
+        default; its error stays in every later Hamiltonian)."""
+        self._check(self.L.tsc_set_split_renormalization(self.h, 1 if on else 0))
+
     def set_split_wait_limit(self, polls: int):
         """Poll limit of the split kernel's bounded waits (default 1<<20; 0 makes
         every wait give up at once, so the next split call fails with TSC_E_CUDA)."""
@@ -159,7 +164,12 @@ class Context:
         blocksparse.Problem; returns (psi length, algorithmic flops of one
         application, flops executed)."""
         from .blocksparse import pack
-        nprob, ints, data = pack(problems)
+        return self.blocksparse_set_packed(*pack(problems))
+
+    def blocksparse_set_packed(self, nprob, ints, data):
+        """blocksparse_set on problems already in pack()'s layout."""
+        ints = np.ascontiguousarray(ints, np.int32)
+        data = np.ascontiguousarray(data, np.complex128)
         dim, flops, xflops = ctypes.c_longlong(), ctypes.c_double(), ctypes.c_double()
         self._check(self.L.tsc_blocksparse_set(self.h, nprob, _iptr(ints), len(ints), _dptr(data), len(data),
                                                ctypes.byref(dim), ctypes.byref(flops), ctypes.byref(xflops)))
