@@ -319,6 +319,14 @@ int tsc_split_views(tsc_ctx* ctx, long long* bytes, int* views);
  * remove it. */
 int tsc_set_split_renormalization(tsc_ctx* ctx, int on);
 
+/* on = 1 (the default): every Lanczos iteration after the first of a solve
+ * (eigen.f90:65-98: three-term update, Gram_Schmidt_process, normalisation,
+ * H.psi, alpha, the tridiagonal Ritz value and its read-back) is one CUDA graph
+ * launch, the graph built once per solve (updated in place when only its
+ * parameters change) and replayed with the iteration index; the results are
+ * bit-identical to on = 0, which launches every step from the host. */
+int tsc_set_lanczos_graph(tsc_ctx* ctx, int on);
+
 /* Poll limit of every bounded mbarrier wait in the split-precision kernel (no
  * counterpart in the reference; default 1<<20, far above any wait of a healthy
  * launch).  A wait that runs out sets the context's status word and the kernel

@@ -437,6 +437,13 @@ int tsc_set_precision(tsc_ctx* ctx, int mode, double split_tol) {
   });
 }
 
+int tsc_set_lanczos_graph(tsc_ctx* ctx, int on) {
+  return guard(ctx, [&] {
+    if (!ctx->eng) throw Error(TSC_E_STATE, "no engine");
+    ctx->eng->lanczos_graph_ = on != 0;
+  });
+}
+
 int tsc_set_split_renormalization(tsc_ctx* ctx, int on) {
   return guard(ctx, [&] {
     if (!ctx->eng) throw Error(TSC_E_STATE, "no engine");

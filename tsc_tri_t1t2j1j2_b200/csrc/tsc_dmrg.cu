@@ -127,6 +127,8 @@ inline long long absoff(const double2* p) { return (long long)((uintptr_t)p / si
 
 // scalar slots in d_scal
 constexpr int S_ALPHA = 0, S_BETA = 128, S_UV = 256, S_UU = 384, S_RES = 512, S_Z = 520, S_N2 = 700, S_PKT = 704, S_CHK = 712, S_ZR = 768;
+constexpr int S_NRM = 1901;   // norm slot of Engine::normalize
+constexpr int S_IT = 1990;    // the graphed iteration's index (an int in a double slot)
 
 // Density-matrix eigenvalues below this are rounding noise (rho has unit trace).
 constexpr double kZeroWeight = 1e-13;
@@ -199,19 +201,20 @@ void Engine::lanczos_run(double2* d_psi, double lanzero, double rel_tol, bool sp
   double* uu_d = d_scal + S_UU;
   double lastmin = 1024.0, ritzmin = 0.0;
   int iter_out = 0, last = 1;
-  int calls = 0;
+  int calls = 0, eager_calls = 0;   // H.psi calls in all, and those with their own event pair
   // H.psi launches are bracketed by events that are read once, after the solve
   auto do_hpsi = [&](int j) {
-    if ((size_t)(2 * calls + 2) > hpsi_events.size()) {
+    if ((size_t)(2 * eager_calls + 2) > hpsi_events.size()) {
       for (int q = 0; q < 2; ++q) {
         cudaEvent_t e;
         cuda_check(cudaEventCreate(&e), "cudaEventCreate");
         hpsi_events.push_back(e);
       }
     }
-    cuda_check(cudaEventRecord(hpsi_events[2 * calls], st), "event");
+    cuda_check(cudaEventRecord(hpsi_events[2 * eager_calls], st), "event");
     hpsi_form(v(j), v(j + 1), split);
-    cuda_check(cudaEventRecord(hpsi_events[2 * calls + 1], st), "event");
+    cuda_check(cudaEventRecord(hpsi_events[2 * eager_calls + 1], st), "event");
+    eager_calls++;
     calls++;
   };
   auto read_back = [&](int slot, int count) {
@@ -225,6 +228,69 @@ void Engine::lanczos_run(double2* d_psi, double lanzero, double rel_tol, bool sp
     read_back(S_RES, 1);
     return h_scal[S_RES];
   };
+  // One iteration's device work (vector steps, H.psi, tail, packet read-back)
+  // as a CUDA graph, replayed with the index written to pinned memory before
+  // each launch (its first node copies it to the device).  The H.psi reads and
+  // writes two fixed vectors, copied from and to the Krylov block inside the
+  // graph; every step computes what the eager iteration computes, bit for bit.
+  // Built at the first iteration whose H.psi is not an autotuner probe.
+  const bool graphs = lanczos_graph_;
+  std::unique_ptr<DevBuf> gx, gy;
+  bool graph_built = false;
+  double graph_hms = 0.0;
+  int* const d_it = reinterpret_cast<int*>(d_scal + S_IT);
+  int* const h_it = reinterpret_cast<int*>(h_scal + S_IT);
+  auto build_graph = [&]() {
+    gx.reset(new DevBuf((size_t)std::max<long long>(n, 1), st, false));
+    gy.reset(new DevBuf((size_t)std::max<long long>(n, 1), st, false));
+    for (auto* e : {&graph_ev_[0], &graph_ev_[1]})
+      if (!*e) cuda_check(cudaEventCreate(e), "cudaEventCreate");
+    const ItRef W{V.p, ld, 0}, V1{V.p, 0, 0}, X{gx->p, 0, 0}, Y{gy->p, 0, 0}, NEXT{V.p, ld, 1};
+    cudaGraph_t g = nullptr;
+    cuda_check(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "begin capture");
+    try {
+      cuda_check(cudaMemcpyAsync(d_it, h_it, sizeof(int), cudaMemcpyHostToDevice, st), "it h2d");
+      cuda_check(launch_it_update(V.p, ld, a_d, b_d, n, d_it, st), "update");
+      cuda_check(launch_it_dot(W, 0, 0, 1, 1, W, n, d_part, d_scal + S_N2, 0, 0, d_it, st), "norm");
+      cuda_check(launch_it_scale(W, d_scal + S_N2, n, d_it, st), "normalize");
+      cuda_check(launch_it_dot(V1, ld, 1, 0, loop_in, W, n, d_part, uv_d + 1, 0, 0, d_it, st), "uv");
+      cuda_check(launch_it_gs(V.p, ld, uv_d + 1, uu_d + 1, n, d_it, st), "gs");
+      cuda_check(launch_it_dot(W, 0, 0, 1, 1, W, n, d_part, d_scal + S_NRM, 0, 0, d_it, st), "norm");
+      cuda_check(launch_it_scale(W, d_scal + S_NRM, n, d_it, st), "scale");
+      cuda_check(launch_it_dot(W, 0, 0, 1, 1, W, n, d_part, uu_d + 1, 1, 0, d_it, st), "uu");
+      cuda_check(launch_it_copy(X, W, n, d_it, st), "copy in");
+      cuda_check(cudaEventRecord(graph_ev_[0], st), "event");
+      hpsi_form(gx->p, gy->p, split);
+      cuda_check(cudaEventRecord(graph_ev_[1], st), "event");
+      cuda_check(launch_it_copy(NEXT, Y, n, d_it, st), "copy out");
+      cuda_check(launch_it_dot(X, 0, 0, 1, 1, Y, n, d_part, a_d + 1, 1, 0, d_it, st), "alpha");
+      cuda_check(launch_it_tail(d_scal + S_N2, a_d, b_d, d_scal + S_RES, d_scal + S_PKT,
+                                res_tol > 0 ? d_scal + S_ZR : nullptr, d_it, st),
+                 "tail");
+      cuda_check(cudaMemcpyAsync(h_scal + S_PKT, d_scal + S_PKT, 4 * sizeof(double), cudaMemcpyDeviceToHost, st),
+                 "d2h");
+    } catch (...) {
+      cudaStreamEndCapture(st, &g);
+      if (g) cudaGraphDestroy(g);
+      throw;
+    }
+    cuda_check(cudaStreamEndCapture(st, &g), "end capture");
+    // reuse the executable graph of the previous solve when only parameters changed
+    bool updated = false;
+    if (graph_exec_) {
+      cudaGraphExecUpdateResultInfo info;
+      updated = cudaGraphExecUpdate(graph_exec_, g, &info) == cudaSuccess;
+      if (!updated) {
+        cudaGetLastError();
+        cudaGraphExecDestroy(graph_exec_);
+        graph_exec_ = nullptr;
+      }
+    }
+    if (!updated) cuda_check(cudaGraphInstantiate(&graph_exec_, g, 0), "graph instantiate");
+    cudaGraphDestroy(g);
+    graph_built = true;
+  };
+  auto graph_ok = [&]() { return graphs && (split || !(sb.tune_cand >= 0 && !sb.tune_pending)); };
   bool done = false;
   while (iter_out <= loop_out && !done) {
     iter_out++;
@@ -246,23 +312,35 @@ void Engine::lanczos_run(double2* d_psi, double lanzero, double rel_tol, bool sp
       // (eigen.f90:70-74); here that test is applied to the read-back value and
       // the iteration's remaining work (vectors last+1, last+2 and slots last+1)
       // is discarded, which leaves the same state.
-      double2* w = v(last + 1);
-      cuda_check(launch_lanczos_update(w, v(last), last >= 2 ? v(last - 1) : nullptr, a_d + last,
-                                       b_d + (last >= 2 ? last - 1 : 0), n, st),
-                 "update");
-      cuda_check(launch_multi_dot(w, ld, 1, w, n, d_part, d_scal + S_N2, st), "norm");
-      cuda_check(launch_scale(w, d_scal + S_N2, n, 1, st), "normalize");
-      // Gram_Schmidt_process against v(1..last) (block.f90:1251-1289)
-      cuda_check(launch_multi_dot(v(1), ld, last, w, n, d_part, uv_d + 1, st), "uv");
-      cuda_check(launch_gs_subtract(w, v(1), ld, last, uv_d + 1, uu_d + 1, n, st), "gs");
-      normalize(w, n);
-      cuda_check(launch_multi_dot(w, ld, 1, w, n, d_part, uu_d + last + 1, st), "uu");
-      do_hpsi(last + 1);
-      cuda_check(launch_multi_dot(v(last + 1), ld, 1, v(last + 2), n, d_part, a_d + last + 1, st), "alpha");
-      cuda_check(launch_lanczos_tail(d_scal + S_N2, a_d, b_d, last + 1, d_scal + S_RES, d_scal + S_PKT,
-                                     res_tol > 0 ? d_scal + S_ZR : nullptr, st),
-                 "tail");
-      read_back(S_PKT, 4);
+      if (graph_ok()) {
+        if (!graph_built) build_graph();
+        *h_it = last;
+        cuda_check(cudaGraphLaunch(graph_exec_, st), "graph launch");
+        cuda_check(cudaStreamSynchronize(st), "sync");
+        tune_observe();
+        float ms = 0.f;
+        cuda_check(cudaEventElapsedTime(&ms, graph_ev_[0], graph_ev_[1]), "event time");
+        graph_hms += ms;
+        calls++;
+      } else {
+        double2* w = v(last + 1);
+        cuda_check(launch_lanczos_update(w, v(last), last >= 2 ? v(last - 1) : nullptr, a_d + last,
+                                         b_d + (last >= 2 ? last - 1 : 0), n, st),
+                   "update");
+        cuda_check(launch_multi_dot(w, ld, 1, w, n, d_part, d_scal + S_N2, st), "norm");
+        cuda_check(launch_scale(w, d_scal + S_N2, n, 1, st), "normalize");
+        // Gram_Schmidt_process against v(1..last) (block.f90:1251-1289)
+        cuda_check(launch_multi_dot(v(1), ld, last, w, n, d_part, uv_d + 1, st), "uv");
+        cuda_check(launch_gs_subtract(w, v(1), ld, last, uv_d + 1, uu_d + 1, n, st), "gs");
+        normalize(w, n);
+        cuda_check(launch_multi_dot(w, ld, 1, w, n, d_part, uu_d + last + 1, st), "uu");
+        do_hpsi(last + 1);
+        cuda_check(launch_multi_dot(v(last + 1), ld, 1, v(last + 2), n, d_part, a_d + last + 1, st), "alpha");
+        cuda_check(launch_lanczos_tail(d_scal + S_N2, a_d, b_d, last + 1, d_scal + S_RES, d_scal + S_PKT,
+                                       res_tol > 0 ? d_scal + S_ZR : nullptr, st),
+                   "tail");
+        read_back(S_PKT, 4);
+      }
       const double beta_last = std::sqrt(h_scal[S_PKT + 1]);
       if (std::fabs(beta_last) <= lanzero) {
         conv = true;
@@ -301,8 +379,8 @@ void Engine::lanczos_run(double2* d_psi, double lanzero, double rel_tol, bool sp
   cuda_check(launch_combine(d_psi, v(1), ld, last, d_scal + S_Z, n, st), "combine");
   normalize(d_psi, n);
   cuda_check(cudaStreamSynchronize(st), "sync");
-  double hms = 0.0;
-  for (int c = 0; c < calls; ++c) {
+  double hms = graph_hms;
+  for (int c = 0; c < eager_calls; ++c) {
     float ms = 0.f;
     cuda_check(cudaEventElapsedTime(&ms, hpsi_events[2 * c], hpsi_events[2 * c + 1]), "event time");
     hms += ms;

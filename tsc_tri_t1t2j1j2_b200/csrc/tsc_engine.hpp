@@ -353,6 +353,10 @@ class Engine {
   // split form only: the U^H O U renormalisation of block growth on the split
   // kernel too (off by default: its ~1e-7 relative error stays in every later H)
   bool split_renorm_ = false;
+  // Lanczos iterations replayed as one CUDA graph per solve (on by default)
+  bool lanczos_graph_ = true;
+  cudaGraphExec_t graph_exec_ = nullptr;   // reused across solves through cudaGraphExecUpdate
+  cudaEvent_t graph_ev_[2] = {nullptr, nullptr};
   bool in_warmup_ = false;    // set while the warm-up (infinite-lattice) steps run
 
   // Autotuner of the FP64 H.psi schedule: for each size class (log2 of the

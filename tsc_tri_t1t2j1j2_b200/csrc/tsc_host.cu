@@ -423,6 +423,9 @@ Engine::~Engine() {
   } catch (...) {
   }
   if (h_scal) cudaFreeHost(h_scal);
+  if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
+  for (cudaEvent_t e : graph_ev_)
+    if (e) cudaEventDestroy(e);
   if (ev0) cudaEventDestroy(ev0);
   if (ev1) cudaEventDestroy(ev1);
   for (cudaEvent_t e : hpsi_events) cudaEventDestroy(e);

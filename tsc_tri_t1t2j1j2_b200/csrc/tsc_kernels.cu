@@ -619,6 +619,147 @@ __global__ void phase_fix_kernel(double2* __restrict__ U, int rows) {
   }
 }
 
+// ---- the same vector steps with the Lanczos index read on the device ---------------
+// For a CUDA graph of one Lanczos iteration, replayed with a different index
+// each time: *it is `last` (1-based, as eigen.f90), and a vector reference
+// {base, ld, add} means base + (*it + add) * ld (ld = 0: base itself).
+__device__ __forceinline__ double2* vref(double2* base, long long ld, int add, const int* it) {
+  return ld ? base + (long long)(*it + add) * ld : base;
+}
+
+__global__ void it_update_kernel(double2* __restrict__ V, long long ld, const double* __restrict__ alpha,
+                                 const double* __restrict__ beta, long long n, const int* __restrict__ it) {
+  const int last = *it;
+  double2* w = V + (long long)last * ld;
+  const double2* v = V + (long long)(last - 1) * ld;
+  const double2* vprev = last >= 2 ? V + (long long)(last - 2) * ld : nullptr;
+  const double a = alpha[last];
+  const double b = last >= 2 ? beta[last - 1] : 0.0;
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+    double2 x = w[e], p = v[e];
+    x.x = x.x - a * p.x;
+    x.y = x.y - a * p.y;
+    if (vprev) {
+      double2 q = vprev[e];
+      x.x = x.x - b * q.x;
+      x.y = x.y - b * q.y;
+    }
+    w[e] = x;
+  }
+}
+
+// partial sums of Re<x_j, y>, j < nvec = (nvec_it ? *it : 0) + nvec_add, x_j = X + j * xs
+__global__ void it_dot_partial(double2* X, long long xld, int xadd, long long xs, int nvec_it, int nvec_add,
+                               double2* Y, long long yld, int yadd, long long n, double* __restrict__ partial,
+                               int nblk, const int* __restrict__ it) {
+  __shared__ double red[VB / 32];
+  const double2* x0 = vref(X, xld, xadd, it);
+  const double2* y = vref(Y, yld, yadd, it);
+  const int nvec = (nvec_it ? *it : 0) + nvec_add;
+  const long long beg = (long long)blockIdx.x * VCHUNK;
+  const long long end = beg + VCHUNK < n ? beg + VCHUNK : n;
+  for (int j = 0; j < nvec; ++j) {
+    const double2* x = x0 + (long long)j * xs;
+    double acc = 0.0;
+    for (long long e = beg + threadIdx.x; e < end; e += VB) {
+      double2 a = x[e], b = y[e];
+      acc = fma(a.x, b.x, acc);
+      acc = fma(a.y, b.y, acc);
+    }
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double sacc = 0.0;
+      for (int w = 0; w < VB / 32; ++w) sacc += red[w];
+      partial[(long long)j * nblk + blockIdx.x] = sacc;
+    }
+    __syncthreads();
+  }
+}
+
+// out[(out_it ? *it : 0) + out_add + j] = sum of the partials of j, for j < nvec (one block per j)
+__global__ void it_dot_final(const double* __restrict__ partial, int nblk, int nvec_it, int nvec_add,
+                             double* __restrict__ out, int out_it, int out_add, const int* __restrict__ it) {
+  const int j = blockIdx.x;
+  if (j >= (nvec_it ? *it : 0) + nvec_add) return;
+  __shared__ double red[32];
+  double acc = 0.0;
+  for (int b = threadIdx.x; b < nblk; b += blockDim.x) acc += partial[(long long)j * nblk + b];
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double sacc = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) sacc += red[w];
+    out[(out_it ? *it : 0) + out_add + j] = sacc;
+  }
+}
+
+__global__ void it_scale_kernel(double2* W, long long wld, int wadd, const double* __restrict__ norm2, long long n,
+                                const int* __restrict__ it) {
+  double2* w = vref(W, wld, wadd, it);
+  const double s = sqrt(*norm2);
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+    double2 x = w[e];
+    x.x = x.x / s;
+    x.y = x.y / s;
+    w[e] = x;
+  }
+}
+
+// w = v(last+1) - sum_{j<last} (uv_j/uu_j) v(j+1)
+__global__ void it_gs_kernel(double2* __restrict__ V, long long ld, const double* __restrict__ uv,
+                             const double* __restrict__ uu, long long n, const int* __restrict__ it) {
+  const int nvec = *it;
+  double2* w = V + (long long)nvec * ld;
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+    double tr = 0.0, tim = 0.0;
+    for (int j = 0; j < nvec; ++j) {
+      const double c = uv[j] / uu[j];
+      double2 x = V[(long long)j * ld + e];
+      tr = tr + c * x.x;
+      tim = tim + c * x.y;
+    }
+    double2 x = w[e];
+    x.x = x.x - tr;
+    x.y = x.y - tim;
+    w[e] = x;
+  }
+}
+
+__global__ void it_copy_kernel(double2* D, long long dld, int dadd, double2* S, long long sld, int sadd, long long n,
+                               const int* __restrict__ it) {
+  double2* d = vref(D, dld, dadd, it);
+  const double2* src = vref(S, sld, sadd, it);
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x)
+    d[e] = src[e];
+}
+
+__global__ void it_tail_kernel(const double* __restrict__ n2, double* __restrict__ alpha, double* __restrict__ beta,
+                               double* __restrict__ res, double* __restrict__ packet, double* __restrict__ zbuf,
+                               const int* __restrict__ it) {
+  __shared__ double sd[128], se[128];
+  const int k = *it + 1;
+  if (k < 1 || k > 127) return;
+  const int lane = threadIdx.x & 31;
+  const double b = sqrt(n2[0]);
+  for (int i = lane; i < k; i += 32) {
+    sd[i] = alpha[i + 1];
+    se[i] = (i + 1 < k - 1) ? beta[i + 1] : (i + 1 == k - 1 ? b : 0.0);
+  }
+  __syncwarp();
+  if (lane == 0) beta[k - 1] = b;
+  tridiag_lowest_warp(sd, se, k, zbuf ? 1 : 0, res, zbuf);
+  __syncwarp();
+  if (lane == 0) {
+    packet[0] = res[0];
+    packet[1] = n2[0];
+    packet[2] = alpha[k];
+    packet[3] = zbuf ? fabs(zbuf[k - 1]) : 0.0;
+  }
+}
+
 inline int grid_for(long long n) {
   long long b = (n + VB - 1) / VB;
   if (b > 148 * 16) b = 148 * 16;
@@ -713,6 +854,45 @@ cudaError_t launch_tridiag_lowest(const double* d, const double* e, int n, int w
                                   cudaStream_t st) {
   if (n < 1 || n > 127) return cudaErrorInvalidValue;
   tridiag_lowest_kernel<<<1, 32, 0, st>>>(d, e, n, want_vec, res, z);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_it_update(double2* V, long long ld, const double* alpha, const double* beta, long long n,
+                             const int* it, cudaStream_t st) {
+  it_update_kernel<<<grid_for(n), VB, 0, st>>>(V, ld, alpha, beta, n, it);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_it_dot(ItRef x, long long xs, int nvec_it, int nvec_add, int nvec_max, ItRef y, long long n,
+                          double* partial, double* out, int out_it, int out_add, const int* it, cudaStream_t st) {
+  int nblk = (int)((n + VCHUNK - 1) / VCHUNK);
+  if (nblk < 1) nblk = 1;
+  if (nvec_max <= 0) return cudaSuccess;
+  it_dot_partial<<<nblk, VB, 0, st>>>(x.base, x.ld, x.add, xs, nvec_it, nvec_add, y.base, y.ld, y.add, n, partial,
+                                      nblk, it);
+  it_dot_final<<<nvec_max, 256, 0, st>>>(partial, nblk, nvec_it, nvec_add, out, out_it, out_add, it);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_it_scale(ItRef w, const double* norm2, long long n, const int* it, cudaStream_t st) {
+  it_scale_kernel<<<grid_for(n), VB, 0, st>>>(w.base, w.ld, w.add, norm2, n, it);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_it_gs(double2* V, long long ld, const double* uv, const double* uu, long long n, const int* it,
+                         cudaStream_t st) {
+  it_gs_kernel<<<grid_for(n), VB, 0, st>>>(V, ld, uv, uu, n, it);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_it_copy(ItRef dst, ItRef src, long long n, const int* it, cudaStream_t st) {
+  it_copy_kernel<<<grid_for(n), VB, 0, st>>>(dst.base, dst.ld, dst.add, src.base, src.ld, src.add, n, it);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_it_tail(const double* n2, double* alpha, double* beta, double* res, double* packet, double* zbuf,
+                           const int* it, cudaStream_t st) {
+  it_tail_kernel<<<1, 32, 0, st>>>(n2, alpha, beta, res, packet, zbuf, it);
   return cudaGetLastError();
 }
 

@@ -164,4 +164,28 @@ cudaError_t launch_tridiag_lowest(const double* d, const double* e, int n, int w
 cudaError_t launch_lanczos_tail(const double* n2, double* alpha, double* beta, int k, double* res, double* packet,
                                 double* zbuf, cudaStream_t st);
 
+// ---- the Lanczos iteration's vector steps with the index read on the device --------
+// (replayable as one CUDA graph: *it = last, the 1-based Lanczos index of
+// eigen.f90).  An ItRef {base, ld, add} is base + (*it + add) * ld, or base when ld = 0.
+struct ItRef {
+  double2* base;
+  long long ld;
+  int add;
+};
+// w = v(last+1) -= alpha_last v(last) + beta_(last-1) v(last-1), V = v(1), vectors ld apart
+cudaError_t launch_it_update(double2* V, long long ld, const double* alpha, const double* beta, long long n,
+                             const int* it, cudaStream_t st);
+// out[(out_it ? last : 0) + out_add + j] = Re<x + j*xs, y> for j < (nvec_it ? last : 0) + nvec_add
+// (at most nvec_max); partial holds nvec_max * ceil(n / 8192) doubles
+cudaError_t launch_it_dot(ItRef x, long long xs, int nvec_it, int nvec_add, int nvec_max, ItRef y, long long n,
+                          double* partial, double* out, int out_it, int out_add, const int* it, cudaStream_t st);
+cudaError_t launch_it_scale(ItRef w, const double* norm2, long long n, const int* it, cudaStream_t st);
+// v(last+1) -= sum_{j<last} (uv_j / uu_j) v(j+1)   (Gram_Schmidt_process)
+cudaError_t launch_it_gs(double2* V, long long ld, const double* uv, const double* uu, long long n, const int* it,
+                         cudaStream_t st);
+cudaError_t launch_it_copy(ItRef dst, ItRef src, long long n, const int* it, cudaStream_t st);
+// launch_lanczos_tail with k = last + 1
+cudaError_t launch_it_tail(const double* n2, double* alpha, double* beta, double* res, double* packet, double* zbuf,
+                           const int* it, cudaStream_t st);
+
 }  // namespace tsc

@@ -118,6 +118,11 @@ class Context:
         lanzero, eigen.f90:101)."""
         self._check(self.L.tsc_set_split_refinement(self.h, float(residual_factor)))
 
+    def set_lanczos_graph(self, on: bool):
+        """Lanczos iterations as CUDA-graph replays (default on; off launches every
+        step from the host; results bit-identical)."""
+        self._check(self.L.tsc_set_lanczos_graph(self.h, 1 if on else 0))
+
     def set_split_renormalization(self, on: bool):
         """Split form only: U^H O U of block growth on the split kernel too (off by
         default; its error stays in every later Hamiltonian)."""
