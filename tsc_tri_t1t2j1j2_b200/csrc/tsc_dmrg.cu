@@ -249,26 +249,27 @@ void Engine::lanczos_run(double2* d_psi, double lanzero, double rel_tol, bool sp
     cudaGraph_t g = nullptr;
     cuda_check(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "begin capture");
     try {
-      cuda_check(cudaMemcpyAsync(d_it, h_it, sizeof(int), cudaMemcpyHostToDevice, st), "it h2d");
-      cuda_check(launch_it_update(V.p, ld, a_d, b_d, n, d_it, st), "update");
-      cuda_check(launch_it_dot(W, 0, 0, 1, 1, W, n, d_part, d_scal + S_N2, 0, 0, d_it, st), "norm");
-      cuda_check(launch_it_scale(W, d_scal + S_N2, n, d_it, st), "normalize");
-      cuda_check(launch_it_dot(V1, ld, 1, 0, loop_in, W, n, d_part, uv_d + 1, 0, 0, d_it, st), "uv");
-      cuda_check(launch_it_gs(V.p, ld, uv_d + 1, uu_d + 1, n, d_it, st), "gs");
-      cuda_check(launch_it_dot(W, 0, 0, 1, 1, W, n, d_part, d_scal + S_NRM, 0, 0, d_it, st), "norm");
-      cuda_check(launch_it_scale(W, d_scal + S_NRM, n, d_it, st), "scale");
-      cuda_check(launch_it_dot(W, 0, 0, 1, 1, W, n, d_part, uu_d + 1, 1, 0, d_it, st), "uu");
-      cuda_check(launch_it_copy(X, W, n, d_it, st), "copy in");
-      cuda_check(cudaEventRecord(graph_ev_[0], st), "event");
+      cuda_check(cudaMemcpyAsync(d_it, h_it, sizeof(int), cudaMemcpyHostToDevice, st), "graph it h2d");
+      cuda_check(launch_it_update(V.p, ld, a_d, b_d, n, d_it, st), "graph update");
+      cuda_check(launch_it_dot(W, 0, 0, 1, 1, W, n, d_part, d_scal + S_N2, 0, 0, d_it, st), "graph norm");
+      cuda_check(launch_it_scale(W, d_scal + S_N2, n, d_it, st), "graph normalize");
+      cuda_check(launch_it_dot(V1, ld, 1, 0, loop_in, W, n, d_part, uv_d + 1, 0, 0, d_it, st), "graph uv");
+      cuda_check(launch_it_gs(V.p, ld, uv_d + 1, uu_d + 1, n, d_it, st), "graph gs");
+      cuda_check(launch_it_dot(W, 0, 0, 1, 1, W, n, d_part, d_scal + S_NRM, 0, 0, d_it, st), "graph norm of w");
+      cuda_check(launch_it_scale(W, d_scal + S_NRM, n, d_it, st), "graph scale");
+      cuda_check(launch_it_dot(W, 0, 0, 1, 1, W, n, d_part, uu_d + 1, 1, 0, d_it, st), "graph uu");
+      cuda_check(launch_it_copy(X, W, n, d_it, st), "graph copy in");
+      // external records: event nodes of the graph, readable after each replay
+      cuda_check(cudaEventRecordWithFlags(graph_ev_[0], st, cudaEventRecordExternal), "graph event");
       hpsi_form(gx->p, gy->p, split);
-      cuda_check(cudaEventRecord(graph_ev_[1], st), "event");
-      cuda_check(launch_it_copy(NEXT, Y, n, d_it, st), "copy out");
-      cuda_check(launch_it_dot(X, 0, 0, 1, 1, Y, n, d_part, a_d + 1, 1, 0, d_it, st), "alpha");
+      cuda_check(cudaEventRecordWithFlags(graph_ev_[1], st, cudaEventRecordExternal), "graph event");
+      cuda_check(launch_it_copy(NEXT, Y, n, d_it, st), "graph copy out");
+      cuda_check(launch_it_dot(X, 0, 0, 1, 1, Y, n, d_part, a_d + 1, 1, 0, d_it, st), "graph alpha");
       cuda_check(launch_it_tail(d_scal + S_N2, a_d, b_d, d_scal + S_RES, d_scal + S_PKT,
                                 res_tol > 0 ? d_scal + S_ZR : nullptr, d_it, st),
-                 "tail");
+                 "graph tail");
       cuda_check(cudaMemcpyAsync(h_scal + S_PKT, d_scal + S_PKT, 4 * sizeof(double), cudaMemcpyDeviceToHost, st),
-                 "d2h");
+                 "graph d2h");
     } catch (...) {
       cudaStreamEndCapture(st, &g);
       if (g) cudaGraphDestroy(g);
@@ -327,7 +328,7 @@ void Engine::lanczos_run(double2* d_psi, double lanzero, double rel_tol, bool sp
         cuda_check(launch_lanczos_update(w, v(last), last >= 2 ? v(last - 1) : nullptr, a_d + last,
                                          b_d + (last >= 2 ? last - 1 : 0), n, st),
                    "update");
-        cuda_check(launch_multi_dot(w, ld, 1, w, n, d_part, d_scal + S_N2, st), "norm");
+        cuda_check(launch_multi_dot(w, ld, 1, w, n, d_part, d_scal + S_N2, st), "iteration norm");
         cuda_check(launch_scale(w, d_scal + S_N2, n, 1, st), "normalize");
         // Gram_Schmidt_process against v(1..last) (block.f90:1251-1289)
         cuda_check(launch_multi_dot(v(1), ld, last, w, n, d_part, uv_d + 1, st), "uv");

@@ -999,7 +999,7 @@ DBlock Engine::copy_block(const DBlock& b) {
 }
 
 double Engine::wave_norm2(const double2* d, long long n) {
-  cuda_check(launch_multi_dot(d, 0, 1, d, n, d_red, d_scal + 1900, st), "norm");
+  cuda_check(launch_multi_dot(d, 0, 1, d, n, d_red, d_scal + 1900, st), "wave norm");
   cuda_check(cudaMemcpyAsync(h_scal + 1900, d_scal + 1900, sizeof(double), cudaMemcpyDeviceToHost, st), "d2h");
   cuda_check(cudaStreamSynchronize(st), "sync");
   return h_scal[1900];
@@ -1007,7 +1007,7 @@ double Engine::wave_norm2(const double2* d, long long n) {
 
 void Engine::normalize(double2* d, long long n) {
   if (n <= 0) return;
-  cuda_check(launch_multi_dot(d, 0, 1, d, n, d_red, d_scal + 1901, st), "norm");
+  cuda_check(launch_multi_dot(d, 0, 1, d, n, d_red, d_scal + 1901, st), "normalize norm");
   cuda_check(launch_scale(d, d_scal + 1901, n, 1, st), "scale");
 }
 
