@@ -327,6 +327,17 @@ int tsc_set_split_renormalization(tsc_ctx* ctx, int on);
  * bit-identical to on = 0, which launches every step from the host. */
 int tsc_set_lanczos_graph(tsc_ctx* ctx, int on);
 
+/* Split form: shared = 1 (the default) slices every operator sub-block once and
+ * lets the kernel's epilogue apply each term's coefficient; shared = 0 slices one
+ * copy per term with its coefficient folded in (~2 % faster H.psi, 4.5x the
+ * memory of the operator slices: 14.3 GB against 3.2 GB on the YC4x24 m=4000
+ * superblock).  Applies from the next superblock set on. */
+int tsc_set_split_view_sharing(tsc_ctx* ctx, int shared);
+/* Iterations replayed as graphs since the context was created, and captures that
+ * failed (the iteration then ran eagerly and graphs stayed off for the context);
+ * reason (may be NULL) receives the last failure's message, NUL-terminated. */
+int tsc_lanczos_graph_stats(tsc_ctx* ctx, long long* replays, long long* fallbacks, char* reason, int reason_cap);
+
 /* Poll limit of every bounded mbarrier wait in the split-precision kernel (no
  * counterpart in the reference; default 1<<20, far above any wait of a healthy
  * launch).  A wait that runs out sets the context's status word and the kernel

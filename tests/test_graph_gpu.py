@@ -15,9 +15,16 @@ def run(mode, graph):
     try:
         ctx.set_precision(mode, 1e-11)
         ctx.set_lanczos_graph(graph)
-        return ctx.get_ground_state(**RUN)
+        steps = ctx.get_ground_state(**RUN)
+        stats = ctx.lanczos_graph_stats()
     finally:
         ctx.close()
+    if graph:   # the graphed run really replayed its iterations
+        assert stats["fallbacks"] == 0, stats["reason"]
+        assert stats["replays"] > len(steps)
+    else:
+        assert stats["replays"] == 0
+    return steps
 
 
 @pytest.mark.gpu

@@ -23,7 +23,8 @@ EXPORTED = [
     "tsc_hpsi_stats", "tsc_stream", "tsc_hpsi_noalloc", "tsc_set_precision", "tsc_set_split_wait_limit",
     "tsc_set_resident_limit", "tsc_spill_stats", "tsc_split_views",
     "tsc_checkpoint_write", "tsc_checkpoint_read", "tsc_set_split_refinement",
-    "tsc_set_split_renormalization", "tsc_set_lanczos_graph",
+    "tsc_set_split_renormalization", "tsc_set_lanczos_graph", "tsc_lanczos_graph_stats",
+    "tsc_set_split_view_sharing",
     "tsc_blocksparse_set", "tsc_blocksparse_apply", "tsc_measure_density", "tsc_measure_density_cor", "tsc_measure_correlation", "tsc_measure_pair_correlation",
     "tsc_set_autotune",
     "tsc_autotune_table", "tsc_autotune_superblock",
@@ -103,6 +104,8 @@ def load():
     L.tsc_set_split_refinement.argtypes = [c_void, c_double]
     L.tsc_set_split_renormalization.argtypes = [c_void, c_int]
     L.tsc_set_lanczos_graph.argtypes = [c_void, c_int]
+    L.tsc_set_split_view_sharing.argtypes = [c_void, c_int]
+    L.tsc_lanczos_graph_stats.argtypes = [c_void, P(c_ll), P(c_ll), ctypes.c_char_p, c_int]
     L.tsc_checkpoint_read.argtypes = [c_void, ctypes.c_char_p]
     L.tsc_spill_stats.argtypes = [c_void, P(c_ll), P(c_ll), P(c_double), P(c_double), P(c_ll), P(c_ll)]
     L.tsc_blocksparse_set.argtypes = [c_void, c_int, ctypes.POINTER(c_int), c_ll, ctypes.POINTER(c_double), c_ll,

@@ -437,10 +437,31 @@ int tsc_set_precision(tsc_ctx* ctx, int mode, double split_tol) {
   });
 }
 
+int tsc_set_split_view_sharing(tsc_ctx* ctx, int shared) {
+  return guard(ctx, [&] {
+    if (!ctx->eng) throw Error(TSC_E_STATE, "no engine");
+    ctx->eng->split_shared_views_ = shared != 0;
+  });
+}
+
 int tsc_set_lanczos_graph(tsc_ctx* ctx, int on) {
   return guard(ctx, [&] {
     if (!ctx->eng) throw Error(TSC_E_STATE, "no engine");
     ctx->eng->lanczos_graph_ = on != 0;
+  });
+}
+
+int tsc_lanczos_graph_stats(tsc_ctx* ctx, long long* replays, long long* fallbacks, char* reason, int reason_cap) {
+  return guard(ctx, [&] {
+    if (!ctx->eng) throw Error(TSC_E_STATE, "no engine");
+    Engine& E = *ctx->eng;
+    if (replays) *replays = E.graph_replays_;
+    if (fallbacks) *fallbacks = E.graph_fallbacks_;
+    if (reason && reason_cap > 0) {
+      const size_t n = std::min<size_t>((size_t)reason_cap - 1, E.graph_fallback_reason_.size());
+      std::memcpy(reason, E.graph_fallback_reason_.data(), n);
+      reason[n] = 0;
+    }
   });
 }
 

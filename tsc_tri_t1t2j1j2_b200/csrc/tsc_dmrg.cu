@@ -240,14 +240,17 @@ void Engine::lanczos_run(double2* d_psi, double lanzero, double rel_tol, bool sp
   double graph_hms = 0.0;
   int* const d_it = reinterpret_cast<int*>(d_scal + S_IT);
   int* const h_it = reinterpret_cast<int*>(h_scal + S_IT);
-  auto build_graph = [&]() {
+  // false: the capture failed (the iteration then runs eagerly and graphs stay
+  // off for this engine; the eager iteration computes the same numbers)
+  auto build_graph = [&]() -> bool {
     gx.reset(new DevBuf((size_t)std::max<long long>(n, 1), st, false));
     gy.reset(new DevBuf((size_t)std::max<long long>(n, 1), st, false));
     for (auto* e : {&graph_ev_[0], &graph_ev_[1]})
       if (!*e) cuda_check(cudaEventCreate(e), "cudaEventCreate");
     const ItRef W{V.p, ld, 0}, V1{V.p, 0, 0}, X{gx->p, 0, 0}, Y{gy->p, 0, 0}, NEXT{V.p, ld, 1};
     cudaGraph_t g = nullptr;
-    cuda_check(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "begin capture");
+    std::shared_lock<std::shared_mutex> capturing(capture_mutex());
+    cuda_check(cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed), "graph begin capture");
     try {
       cuda_check(cudaMemcpyAsync(d_it, h_it, sizeof(int), cudaMemcpyHostToDevice, st), "graph it h2d");
       cuda_check(launch_it_update(V.p, ld, a_d, b_d, n, d_it, st), "graph update");
@@ -270,12 +273,23 @@ void Engine::lanczos_run(double2* d_psi, double lanzero, double rel_tol, bool sp
                  "graph tail");
       cuda_check(cudaMemcpyAsync(h_scal + S_PKT, d_scal + S_PKT, 4 * sizeof(double), cudaMemcpyDeviceToHost, st),
                  "graph d2h");
-    } catch (...) {
+    } catch (std::exception& e) {
       cudaStreamEndCapture(st, &g);
       if (g) cudaGraphDestroy(g);
-      throw;
+      cudaGetLastError();
+      graph_fallbacks_++;
+      graph_fallback_reason_ = e.what();
+      lanczos_graph_ = false;
+      return false;
     }
-    cuda_check(cudaStreamEndCapture(st, &g), "end capture");
+    if (cudaStreamEndCapture(st, &g) != cudaSuccess || !g) {
+      cudaGetLastError();
+      if (g) cudaGraphDestroy(g);
+      graph_fallbacks_++;
+      graph_fallback_reason_ = "capture invalidated";
+      lanczos_graph_ = false;
+      return false;
+    }
     // reuse the executable graph of the previous solve when only parameters changed
     bool updated = false;
     if (graph_exec_) {
@@ -290,8 +304,9 @@ void Engine::lanczos_run(double2* d_psi, double lanzero, double rel_tol, bool sp
     if (!updated) cuda_check(cudaGraphInstantiate(&graph_exec_, g, 0), "graph instantiate");
     cudaGraphDestroy(g);
     graph_built = true;
+    return true;
   };
-  auto graph_ok = [&]() { return graphs && (split || !(sb.tune_cand >= 0 && !sb.tune_pending)); };
+  auto graph_ok = [&]() { return graphs && lanczos_graph_ && (split || !(sb.tune_cand >= 0 && !sb.tune_pending)); };
   bool done = false;
   while (iter_out <= loop_out && !done) {
     iter_out++;
@@ -313,8 +328,7 @@ void Engine::lanczos_run(double2* d_psi, double lanzero, double rel_tol, bool sp
       // (eigen.f90:70-74); here that test is applied to the read-back value and
       // the iteration's remaining work (vectors last+1, last+2 and slots last+1)
       // is discarded, which leaves the same state.
-      if (graph_ok()) {
-        if (!graph_built) build_graph();
+      if (graph_ok() && (graph_built || build_graph())) {
         *h_it = last;
         cuda_check(cudaGraphLaunch(graph_exec_, st), "graph launch");
         cuda_check(cudaStreamSynchronize(st), "sync");
@@ -322,6 +336,7 @@ void Engine::lanczos_run(double2* d_psi, double lanzero, double rel_tol, bool sp
         float ms = 0.f;
         cuda_check(cudaEventElapsedTime(&ms, graph_ev_[0], graph_ev_[1]), "event time");
         graph_hms += ms;
+        graph_replays_++;
         calls++;
       } else {
         double2* w = v(last + 1);
@@ -478,7 +493,10 @@ void Engine::truncation_operator(DBlock& den, int kept_min, int kept_max, double
   double* d_ev = reinterpret_cast<double*>(ev.p);
   DevBuf info((size_t)(nsec + 1) / 4 + 1, st, true);   // one int per sector
   int* d_info = reinterpret_cast<int*>(info.p);
-  if (!eig) eig = std::make_shared<EigLanes>(kEigLanes, device_);
+  if (!eig) {   // handles, streams and workspaces: not while another engine captures a graph
+    std::unique_lock<std::shared_mutex> no_capture(capture_mutex());
+    eig = std::make_shared<EigLanes>(kEigLanes, device_);
+  }
   std::vector<int> order(nsec);
   for (int k = 0; k < nsec; ++k) order[k] = k;
   auto sdim = [&](int k) { return den.sub[k].sdim; };

@@ -12,6 +12,7 @@
 #include <complex>
 #include <map>
 #include <memory>
+#include <shared_mutex>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -28,6 +29,12 @@ struct Error : std::runtime_error {
 };
 
 void cuda_check(cudaError_t e, const char* what);
+
+// Engines of one process share this lock: a stream capture (the Lanczos graph)
+// holds it shared, engine construction and destruction hold it exclusively,
+// because their device-synchronising calls (pinned host memory, pool trims)
+// would invalidate a capture running in another thread.
+std::shared_mutex& capture_mutex();
 
 // ---- device memory -----------------------------------------------------------
 // Device buffer of complex elements, stream-ordered on `st`.  Buffers are carved
@@ -353,10 +360,15 @@ class Engine {
   // split form only: the U^H O U renormalisation of block growth on the split
   // kernel too (off by default: its ~1e-7 relative error stays in every later H)
   bool split_renorm_ = false;
+  // split form: operator views shared by all terms (coefficients in the epilogue)
+  // or, when false, one view per term with its coefficient folded in
+  bool split_shared_views_ = true;
   // Lanczos iterations replayed as one CUDA graph per solve (on by default)
   bool lanczos_graph_ = true;
   cudaGraphExec_t graph_exec_ = nullptr;   // reused across solves through cudaGraphExecUpdate
   cudaEvent_t graph_ev_[2] = {nullptr, nullptr};
+  long long graph_replays_ = 0, graph_fallbacks_ = 0;   // iterations replayed; failed captures
+  std::string graph_fallback_reason_;
   bool in_warmup_ = false;    // set while the warm-up (infinite-lattice) steps run
 
   // Autotuner of the FP64 H.psi schedule: for each size class (log2 of the

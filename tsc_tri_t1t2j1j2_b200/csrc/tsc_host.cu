@@ -16,6 +16,11 @@
 
 namespace tsc {
 
+std::shared_mutex& capture_mutex() {
+  static std::shared_mutex m;
+  return m;
+}
+
 void cuda_check(cudaError_t e, const char* what) {
   if (e != cudaSuccess) throw Error(e == cudaErrorMemoryAllocation ? -5 : -3,
                                     std::string(what) + ": " + cudaGetErrorString(e));
@@ -361,6 +366,7 @@ void Lattice::setup0() {
 
 // ---- engine -------------------------------------------------------------------------
 Engine::Engine(int Nx, int Ny, double t1, double t2, double J1, double J2, int delta, int device) {
+  std::unique_lock<std::shared_mutex> no_capture(capture_mutex());
   if (Nx < 2 || Ny < 2 || Nx * Ny > 1024) throw Error(-1, "lattice size out of range");
   if (delta < 1) throw Error(-1, "delta must be >= 1");
   int ndev = 0;
@@ -408,6 +414,7 @@ void Engine::check_split_fault() {
 }
 
 Engine::~Engine() {
+  std::unique_lock<std::shared_mutex> no_capture(capture_mutex());
   sb = Superblock();
   bs = BlockSparse();
   models_.clear();

@@ -978,7 +978,11 @@ void Engine::build_hpsi_tasks() {
     S.p1s.gterms = S.p1.gterms;
     S.p2s.groups = S.p2.groups;
     S.p2s.gterms = S.p2.gterms;
-    build_split_views(S.p1s, S.p2s, S.sv, st);
+    // shared views (the default): one sliced copy per operator block, the terms'
+    // coefficients applied by the kernel's epilogue; 4.5x less memory than views
+    // with the coefficients folded in (YC4x24 m=4000: 3.2 GB against 14.3 GB)
+    // for ~2 % more H.psi time, and as much less slicing when the superblock is set
+    build_split_views(S.p1s, S.p2s, S.sv, st, split_shared_views_);
     S.p1s.upload_split(st);
     S.p2s.upload_split(st);
     S.p1s.gterms.clear();

@@ -123,6 +123,20 @@ class Context:
         step from the host; results bit-identical)."""
         self._check(self.L.tsc_set_lanczos_graph(self.h, 1 if on else 0))
 
+    def set_split_view_sharing(self, shared: bool):
+        """Split form: one sliced copy per operator block with the coefficients applied
+        per term by the kernel (True, the default) or one copy per term with the
+        coefficient folded in (False: ~2 % faster H.psi, 4.5x the slice memory)."""
+        self._check(self.L.tsc_set_split_view_sharing(self.h, 1 if shared else 0))
+
+    def lanczos_graph_stats(self):
+        """{"replays": iterations replayed as graphs, "fallbacks": failed captures,
+        "reason": the last failure's message}."""
+        r, f = ctypes.c_longlong(), ctypes.c_longlong()
+        buf = ctypes.create_string_buffer(512)
+        self._check(self.L.tsc_lanczos_graph_stats(self.h, ctypes.byref(r), ctypes.byref(f), buf, 512))
+        return {"replays": r.value, "fallbacks": f.value, "reason": buf.value.decode()}
+
     def set_split_renormalization(self, on: bool):
         """Split form only: U^H O U of block growth on the split kernel too (off by
         default; its error stays in every later Hamiltonian)."""
