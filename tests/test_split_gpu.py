@@ -54,8 +54,8 @@ def test_split_lanczos_energy(captured):
 
 @pytest.mark.gpu
 def test_split_hpsi_bench_superblock():
-    """YC4x12 m=1000 superblock: the split H.psi with shared operator views (the
-    default, coefficients applied per term in the epilogue) and with one
+    """YC4x12 m=1000 superblock: the split H.psi with shared operator views
+    (coefficients applied per term in the epilogue) and with one
     coefficient-folded view per term both within 1e-6 of FP64 (3.8e-7 measured);
     the shared views take less than a third of the folded ones' memory."""
     import bench

@@ -440,7 +440,7 @@ int tsc_set_precision(tsc_ctx* ctx, int mode, double split_tol) {
 int tsc_set_split_view_sharing(tsc_ctx* ctx, int shared) {
   return guard(ctx, [&] {
     if (!ctx->eng) throw Error(TSC_E_STATE, "no engine");
-    ctx->eng->split_shared_views_ = shared != 0;
+    ctx->eng->split_shared_views_ = shared < 0 ? -1 : (shared != 0 ? 1 : 0);
   });
 }
 

@@ -978,11 +978,23 @@ void Engine::build_hpsi_tasks() {
     S.p1s.gterms = S.p1.gterms;
     S.p2s.groups = S.p2.groups;
     S.p2s.gterms = S.p2.gterms;
-    // shared views (the default): one sliced copy per operator block, the terms'
-    // coefficients applied by the kernel's epilogue; 4.5x less memory than views
-    // with the coefficients folded in (YC4x24 m=4000: 3.2 GB against 14.3 GB)
-    // for ~2 % more H.psi time, and as much less slicing when the superblock is set
-    build_split_views(S.p1s, S.p2s, S.sv, st, split_shared_views_);
+    // shared views: one sliced copy per operator block, the terms' coefficients
+    // applied by the kernel's epilogue; ~4.5x less memory than views with the
+    // coefficients folded in (YC4x24 m=4000: 3.2 GB against 14.3 GB) for ~1-2 %
+    // more H.psi time (segments break at every term).  Automatic choice: shared
+    // once the folded copies (~3.5x the operators' FP64 bytes) would pass 4 GiB.
+    bool shared = split_shared_views_ > 0;
+    if (split_shared_views_ < 0) {
+      double op_bytes = 0.0;
+      for (const DModel* m : {&S.sys, &S.env}) {
+        op_bytes += 16.0 * (double)m->ham.total();
+        for (const OpSet& o : m->sub)
+          for (const DBlock& b : o.op)
+            if (b.buf) op_bytes += 16.0 * (double)b.total();
+      }
+      shared = 3.5 * op_bytes > 4.0 * 1073741824.0;
+    }
+    build_split_views(S.p1s, S.p2s, S.sv, st, shared);
     S.p1s.upload_split(st);
     S.p2s.upload_split(st);
     S.p1s.gterms.clear();

@@ -123,11 +123,12 @@ class Context:
         step from the host; results bit-identical)."""
         self._check(self.L.tsc_set_lanczos_graph(self.h, 1 if on else 0))
 
-    def set_split_view_sharing(self, shared: bool):
+    def set_split_view_sharing(self, shared):
         """Split form: one sliced copy per operator block with the coefficients applied
-        per term by the kernel (True, the default) or one copy per term with the
-        coefficient folded in (False: ~2 % faster H.psi, 4.5x the slice memory)."""
-        self._check(self.L.tsc_set_split_view_sharing(self.h, 1 if shared else 0))
+        per term by the kernel (True), one copy per term with the coefficient folded
+        in (False: 1-2 % faster H.psi, ~4.5x the slice memory), or None (the
+        default) to choose by the superblock's operator memory."""
+        self._check(self.L.tsc_set_split_view_sharing(self.h, -1 if shared is None else (1 if shared else 0)))
 
     def lanczos_graph_stats(self):
         """{"replays": iterations replayed as graphs, "fallbacks": failed captures,
