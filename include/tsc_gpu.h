@@ -327,13 +327,13 @@ int tsc_set_split_renormalization(tsc_ctx* ctx, int on);
  * bit-identical to on = 0, which launches every step from the host. */
 int tsc_set_lanczos_graph(tsc_ctx* ctx, int on);
 
-/* Split form: shared = 1 slices every operator sub-block once and lets the
- * kernel's epilogue apply each term's coefficient; shared = 0 slices one copy
- * per term with its coefficient folded in (1-2 % faster H.psi, ~4.5x the memory
- * of the operator slices: 14.3 GB against 3.2 GB on the YC4x24 m=4000
- * superblock, and more slicing when a superblock is set); shared = -1 (the
- * default) picks shared once the folded copies would pass 4 GiB.  Applies from
- * the next superblock set on. */
+/* Split form: shared = 1 (the default) slices every operator sub-block once and
+ * lets the kernel's epilogue apply each term's coefficient; shared = 0 slices
+ * one copy per term with its coefficient folded in (1-2 % faster H.psi, ~4.5x
+ * the memory of the operator slices: 14.3 GB against 3.2 GB on the YC4x24
+ * m=4000 superblock, and more slicing when a superblock is set); shared = -1
+ * picks shared once the folded copies would pass 4 GiB.  Applies from the next
+ * superblock set on. */
 int tsc_set_split_view_sharing(tsc_ctx* ctx, int shared);
 /* Iterations replayed as graphs since the context was created, and captures that
  * failed (the iteration then ran eagerly and graphs stayed off for the context);

@@ -360,10 +360,10 @@ class Engine {
   // split form only: the U^H O U renormalisation of block growth on the split
   // kernel too (off by default: its ~1e-7 relative error stays in every later H)
   bool split_renorm_ = false;
-  // split form: operator views shared by all terms (1, coefficients in the
-  // epilogue), one view per term with its coefficient folded in (0), or chosen
-  // by the superblock's operator memory (-1, the default)
-  int split_shared_views_ = -1;
+  // split form: operator views shared by all terms (1, the default: coefficients
+  // in the epilogue), one view per term with its coefficient folded in (0), or
+  // chosen by the superblock's operator memory (-1)
+  int split_shared_views_ = 1;
   // Lanczos iterations replayed as one CUDA graph per solve (on by default)
   bool lanczos_graph_ = true;
   cudaGraphExec_t graph_exec_ = nullptr;   // reused across solves through cudaGraphExecUpdate

@@ -978,11 +978,12 @@ void Engine::build_hpsi_tasks() {
     S.p1s.gterms = S.p1.gterms;
     S.p2s.groups = S.p2.groups;
     S.p2s.gterms = S.p2.gterms;
-    // shared views: one sliced copy per operator block, the terms' coefficients
-    // applied by the kernel's epilogue; ~4.5x less memory than views with the
-    // coefficients folded in (YC4x24 m=4000: 3.2 GB against 14.3 GB) for ~1-2 %
-    // more H.psi time (segments break at every term).  Automatic choice: shared
-    // once the folded copies (~3.5x the operators' FP64 bytes) would pass 4 GiB.
+    // shared views (the default): one sliced copy per operator block, the terms'
+    // coefficients applied by the kernel's epilogue; ~4.5x less memory than views
+    // with the coefficients folded in (YC4x24 m=4000: 3.2 GB against 14.3 GB) and
+    // as much less slicing when the superblock is set, for ~1-2 % more H.psi time
+    // (segments break at every term).  Automatic choice (-1): shared once the
+    // folded copies (~3.5x the operators' FP64 bytes) would pass 4 GiB.
     bool shared = split_shared_views_ > 0;
     if (split_shared_views_ < 0) {
       double op_bytes = 0.0;

@@ -125,9 +125,9 @@ class Context:
 
     def set_split_view_sharing(self, shared):
         """Split form: one sliced copy per operator block with the coefficients applied
-        per term by the kernel (True), one copy per term with the coefficient folded
-        in (False: 1-2 % faster H.psi, ~4.5x the slice memory), or None (the
-        default) to choose by the superblock's operator memory."""
+        per term by the kernel (True, the default), one copy per term with the
+        coefficient folded in (False: 1-2 % faster H.psi, ~4.5x the slice memory),
+        or None to choose by the superblock's operator memory."""
         self._check(self.L.tsc_set_split_view_sharing(self.h, -1 if shared is None else (1 if shared else 0)))
 
     def lanczos_graph_stats(self):
