@@ -281,10 +281,12 @@ void* tsc_stream(tsc_ctx* ctx);
  * TSC_SPLIT_BF16: every FP64 operand split into three BF16 slices multiplied
  * on the tensor cores with FP32 accumulators restarted every 128 of the inner
  * dimension and summed in FP64 (a few 1e-7 relative error per H.psi; the
- * operator slices, with the terms' coefficients folded in, are built when the
- * superblock is set); Lanczos iterates on that H.psi until successive Ritz
- * values agree to split_tol relative (<= 0 keeps the current value, 1e-9 at
- * creation), then runs the reference's FP64 iterations from that vector, with
+ * operator slices are built when the superblock is set, see
+ * tsc_set_split_view_sharing); Lanczos iterates on that H.psi until successive
+ * Ritz values agree to split_tol relative (<= 0 keeps the current value, 1e-11
+ * at creation: on YC4x12 whole runs 1e-10, 1e-9 and 1e-8 left more work to the
+ * FP64 iterations and ended farther from FP64), then runs the reference's FP64
+ * iterations from that vector, with
  * the reference's stop unless tsc_set_split_refinement asks for a residual
  * bound, so the energy and vector it returns are FP64 results.  Orthogonalisation, tridiagonal solve,
  * density-matrix eigensolver, renormalisation and wave transforms stay FP64,

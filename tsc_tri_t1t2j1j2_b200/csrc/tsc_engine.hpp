@@ -351,7 +351,7 @@ class Engine {
   // tensor cores, Lanczos finished by FP64 iterations.  Applies from the next
   // superblock set on.
   int precision_ = 0;
-  double split_tol_ = 1e-9;   // relative Ritz-value change that ends the split iterations
+  double split_tol_ = 1e-11;  // relative Ritz-value change that ends the split iterations
   // FP64 iterations that finish a split solve stop when the Ritz residual is
   // <= refine_res_ * sqrt(lanzero); 0 (the default): the reference's own stop
   // (successive Ritz values within lanzero, eigen.f90:101)
