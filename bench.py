@@ -669,12 +669,16 @@ def run_gpu(args):
             "gpu_launches": 2 * args.steps,
             "clocks": r["clocks"],
         }
-        line["split"] = split_leg(torch, dev, sb, max(10, args.steps // 4), gpu_out, model, r["kernel_ms"])
-        if args.config != 2:
+        # side legs only at N = 1: under torchrun the other ranks wait at the closing
+        # barrier, whose process-group timeout the legs' minutes would exceed
+        side = ws == 1
+        if side:
+            line["split"] = split_leg(torch, dev, sb, max(10, args.steps // 4), gpu_out, model, r["kernel_ms"])
+        if side and args.config != 2:
             line["config2_hpsi"] = config2_leg(torch, dev, args.warmup)
-        if not args.no_synthetic:
+        if side and not args.no_synthetic:
             line["config5"] = config5_leg(torch, dev, peak)
-        if not args.no_sweep:
+        if side and not args.no_sweep:
             line["sweep"] = sweep_leg(dev)
             line["sweep_config1"] = config1_leg(dev, ws == 1 and not args.no_cpu)
             line["parameter_points"] = points_leg(dev)
