@@ -321,6 +321,13 @@ int tsc_split_views(tsc_ctx* ctx, long long* bytes, int* views);
  * remove it. */
 int tsc_set_split_renormalization(tsc_ctx* ctx, int on);
 
+/* Split form: the FP64 iterations that finish a split solve stop, with the
+ * reference's test, when successive Ritz values agree to multiplier * lanzero
+ * (1 at creation: the reference's own tolerance; 10 cut a YC4x12 run's FP64
+ * iterations from 1,672 to 1,216 but left its final energy 2.3e-10 from the
+ * FP64 form's, against 3.2e-11 at 1). */
+int tsc_set_split_finish_tolerance(tsc_ctx* ctx, double multiplier);
+
 /* on = 1 (the default): every Lanczos iteration after the first of a solve
  * (eigen.f90:65-98: three-term update, Gram_Schmidt_process, normalisation,
  * H.psi, alpha, the tridiagonal Ritz value and its read-back) is one CUDA graph

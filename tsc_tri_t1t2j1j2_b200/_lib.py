@@ -24,7 +24,7 @@ EXPORTED = [
     "tsc_set_resident_limit", "tsc_spill_stats", "tsc_split_views",
     "tsc_checkpoint_write", "tsc_checkpoint_read", "tsc_set_split_refinement",
     "tsc_set_split_renormalization", "tsc_set_lanczos_graph", "tsc_lanczos_graph_stats",
-    "tsc_set_split_view_sharing",
+    "tsc_set_split_view_sharing", "tsc_set_split_finish_tolerance",
     "tsc_blocksparse_set", "tsc_blocksparse_apply", "tsc_measure_density", "tsc_measure_density_cor", "tsc_measure_correlation", "tsc_measure_pair_correlation",
     "tsc_set_autotune",
     "tsc_autotune_table", "tsc_autotune_superblock",
@@ -105,6 +105,7 @@ def load():
     L.tsc_set_split_renormalization.argtypes = [c_void, c_int]
     L.tsc_set_lanczos_graph.argtypes = [c_void, c_int]
     L.tsc_set_split_view_sharing.argtypes = [c_void, c_int]
+    L.tsc_set_split_finish_tolerance.argtypes = [c_void, c_double]
     L.tsc_lanczos_graph_stats.argtypes = [c_void, P(c_ll), P(c_ll), ctypes.c_char_p, c_int]
     L.tsc_checkpoint_read.argtypes = [c_void, ctypes.c_char_p]
     L.tsc_spill_stats.argtypes = [c_void, P(c_ll), P(c_ll), P(c_double), P(c_double), P(c_ll), P(c_ll)]

@@ -465,6 +465,14 @@ int tsc_lanczos_graph_stats(tsc_ctx* ctx, long long* replays, long long* fallbac
   });
 }
 
+int tsc_set_split_finish_tolerance(tsc_ctx* ctx, double multiplier) {
+  return guard(ctx, [&] {
+    if (!ctx->eng) throw Error(TSC_E_STATE, "no engine");
+    if (!(multiplier > 0.0)) throw Error(TSC_E_ARG, "multiplier must be > 0");
+    ctx->eng->finish_mult_ = multiplier;
+  });
+}
+
 int tsc_set_split_renormalization(tsc_ctx* ctx, int on) {
   return guard(ctx, [&] {
     if (!ctx->eng) throw Error(TSC_E_STATE, "no engine");

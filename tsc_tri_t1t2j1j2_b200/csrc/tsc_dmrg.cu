@@ -176,7 +176,7 @@ void Engine::lanczos(double2* d_psi, double lanzero, int* iters, double* e0, dou
   // FP64 Lanczos from that vector, stopped on the Ritz residual
   // ||H psi - E psi|| <= refine_res_ sqrt(lanzero) (from the tridiagonal, no extra
   // H.psi), or, with refine_res_ = 0, by the reference's own test
-  lanczos_run(d_psi, lanzero, 0.0, false, &it2, e0, &ms2, &c2, refine_res_ * std::sqrt(lanzero));
+  lanczos_run(d_psi, lanzero * finish_mult_, 0.0, false, &it2, e0, &ms2, &c2, refine_res_ * std::sqrt(lanzero));
   last_split_iters = it1;
   last_split_e0 = e_split;
   *iters = it1 + it2;

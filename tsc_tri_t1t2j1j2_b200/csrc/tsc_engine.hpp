@@ -356,6 +356,9 @@ class Engine {
   // <= refine_res_ * sqrt(lanzero); 0 (the default): the reference's own stop
   // (successive Ritz values within lanzero, eigen.f90:101)
   double refine_res_ = 0.0;
+  // the reference's stop of that FP64 finish compares successive Ritz values
+  // with finish_mult_ * lanzero
+  double finish_mult_ = 1.0;
   bool split_now_ = false;    // the current superblock's solve uses the split form
   // split form only: the U^H O U renormalisation of block growth on the split
   // kernel too (off by default: its ~1e-7 relative error stays in every later H)

@@ -123,6 +123,11 @@ class Context:
         step from the host; results bit-identical)."""
         self._check(self.L.tsc_set_lanczos_graph(self.h, 1 if on else 0))
 
+    def set_split_finish_tolerance(self, multiplier: float):
+        """Split form: the FP64 finish stops when successive Ritz values agree to
+        multiplier * lanzero (1: the reference's tolerance)."""
+        self._check(self.L.tsc_set_split_finish_tolerance(self.h, float(multiplier)))
+
     def set_split_view_sharing(self, shared):
         """Split form: one sliced copy per operator block with the coefficients applied
         per term by the kernel (True, the default), one copy per term with the
