@@ -192,6 +192,18 @@ int tsc_set_resident_limit(tsc_ctx* ctx, long long bytes);
  * seconds spent, the bytes now resident and the limit in force. */
 int tsc_spill_stats(tsc_ctx* ctx, long long* spills, long long* restores, double* bytes, double* seconds,
                     long long* resident_bytes, long long* limit_bytes);
+/* Disk tier under the host spill, the reference's own out-of-core storage
+ * (model_to_disk / block_to_disk, block.f90:1715-1900): once the spilled
+ * models' host copies pass host_bytes, the least recently used go to one file
+ * each in directory dir (created by the caller) and come back, through host
+ * memory, when the sweep reads them; each file is removed when its model comes
+ * back or the context is destroyed.  host_bytes < 0 or dir NULL/empty: no disk
+ * tier (the default).  Results are unchanged (the data round-trips exactly). */
+int tsc_set_spill_directory(tsc_ctx* ctx, const char* dir, long long host_bytes);
+/* Models written to and read from the disk tier, bytes moved both ways, wall
+ * seconds, and the host bytes the spilled models hold now. */
+int tsc_disk_spill_stats(tsc_ctx* ctx, long long* writes, long long* reads, double* bytes, double* seconds,
+                         long long* host_bytes);
 
 /* <n_i> of every site in the last ground state of tsc_dmrg_run, sites 1..Nx*Ny
  * in the lattice order (measure_operator_dia with num_elec, measure.f90:3-62,

@@ -40,3 +40,28 @@ def test_spilled_run_is_bit_identical():
         assert g["num_state"] == r["num_state"]
         assert g["trun_err"] == r["trun_err"]
         assert g["lanczos_iters"] == r["lanczos_iters"]
+
+
+@pytest.mark.gpu
+def test_disk_tier_run_is_bit_identical(tmp_path):
+    """Resident limit 0 and host limit 0 with a spill directory: every stored
+    model goes to a file between its uses (the reference's own disk round trip)
+    and the run stays bit-identical to the resident one; the files are gone when
+    the context closes."""
+    ref, _ = run(-1)
+    ctx = Context(device=0, **MODEL)
+    try:
+        ctx.set_autotune(False)
+        ctx.set_resident_limit(0)
+        ctx.set_spill_directory(str(tmp_path), 0)
+        got = ctx.get_ground_state(**RUN)
+        disk = ctx.disk_spill_stats()
+    finally:
+        ctx.close()
+    assert disk["writes"] > 0 and disk["reads"] > 0 and disk["bytes"] > 0
+    assert list(tmp_path.iterdir()) == []
+    assert len(got) == len(ref)
+    for g, r in zip(got, ref):
+        assert g["e0"] == r["e0"]
+        assert g["num_state"] == r["num_state"]
+        assert g["trun_err"] == r["trun_err"]

@@ -21,7 +21,7 @@ EXPORTED = [
     "tsc_density_matrix", "tsc_truncation_operator",
     "tsc_renormalize", "tsc_wave_transform", "tsc_dmrg_run", "tsc_set_capture", "tsc_get_capture",
     "tsc_hpsi_stats", "tsc_stream", "tsc_hpsi_noalloc", "tsc_set_precision", "tsc_set_split_wait_limit",
-    "tsc_set_resident_limit", "tsc_spill_stats", "tsc_split_views",
+    "tsc_set_resident_limit", "tsc_spill_stats", "tsc_set_spill_directory", "tsc_disk_spill_stats", "tsc_split_views",
     "tsc_checkpoint_write", "tsc_checkpoint_read", "tsc_set_split_refinement",
     "tsc_set_split_renormalization", "tsc_set_lanczos_graph", "tsc_lanczos_graph_stats",
     "tsc_set_split_view_sharing", "tsc_set_split_finish_tolerance",
@@ -109,6 +109,8 @@ def load():
     L.tsc_lanczos_graph_stats.argtypes = [c_void, P(c_ll), P(c_ll), ctypes.c_char_p, c_int]
     L.tsc_checkpoint_read.argtypes = [c_void, ctypes.c_char_p]
     L.tsc_spill_stats.argtypes = [c_void, P(c_ll), P(c_ll), P(c_double), P(c_double), P(c_ll), P(c_ll)]
+    L.tsc_set_spill_directory.argtypes = [c_void, ctypes.c_char_p, c_ll]
+    L.tsc_disk_spill_stats.argtypes = [c_void, P(c_ll), P(c_ll), P(c_double), P(c_double), P(c_ll)]
     L.tsc_blocksparse_set.argtypes = [c_void, c_int, ctypes.POINTER(c_int), c_ll, ctypes.POINTER(c_double), c_ll,
                                       ctypes.POINTER(c_ll), ctypes.POINTER(c_double), ctypes.POINTER(c_double)]
     L.tsc_blocksparse_apply.argtypes = [c_void, c_void, c_void, c_int]

@@ -516,6 +516,26 @@ int tsc_set_resident_limit(tsc_ctx* ctx, long long bytes) {
   });
 }
 
+int tsc_set_spill_directory(tsc_ctx* ctx, const char* dir, long long host_bytes) {
+  return guard(ctx, [&] {
+    if (!ctx->eng) throw Error(TSC_E_STATE, "no engine");
+    ctx->eng->model_store().set_disk(dir && *dir ? host_bytes : -1, dir ? std::string(dir) : std::string());
+  });
+}
+
+int tsc_disk_spill_stats(tsc_ctx* ctx, long long* writes, long long* reads, double* bytes, double* seconds,
+                         long long* host_bytes) {
+  return guard(ctx, [&] {
+    if (!ctx->eng) throw Error(TSC_E_STATE, "no engine");
+    ModelStore& m = ctx->eng->model_store();
+    if (writes) *writes = m.disk_writes;
+    if (reads) *reads = m.disk_reads;
+    if (bytes) *bytes = m.disk_bytes;
+    if (seconds) *seconds = m.disk_seconds;
+    if (host_bytes) *host_bytes = m.host_bytes();
+  });
+}
+
 int tsc_spill_stats(tsc_ctx* ctx, long long* spills, long long* restores, double* bytes, double* seconds,
                     long long* resident_bytes, long long* limit_bytes) {
   return guard(ctx, [&] {

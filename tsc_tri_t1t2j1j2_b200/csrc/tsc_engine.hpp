@@ -196,7 +196,8 @@ class ModelStore {
     for (const auto& kv : map_) k.push_back({(int)(kv.first >> 32), (int)(kv.first & 0xffffffff)});
     return k;
   }
-  void clear() { map_.clear(); resident_ = 0; }
+  void clear();   // drops every model (and the files of those on disk)
+  ~ModelStore() { clear(); }
   void bind(cudaStream_t st) { st_ = st; }
   // bytes of device memory the stored models may hold; < 0: default_frac of the device
   void set_limit(long long bytes) { limit_ = bytes; }
@@ -206,12 +207,24 @@ class ModelStore {
   long long resident_bytes() const { return resident_; }
   long long spills = 0, restores = 0;
   double moved_bytes = 0, moved_seconds = 0;
+  // Disk tier: spilled models beyond host_bytes of host memory go to files in
+  // dir (the reference's own out-of-core storage); host_bytes < 0 or an empty
+  // dir: no disk tier (the default).
+  void set_disk(long long host_bytes, const std::string& dir) {
+    host_limit_ = host_bytes;
+    disk_dir_ = dir;
+  }
+  long long host_bytes() const { return host_bytes_; }
+  long long disk_writes = 0, disk_reads = 0;
+  double disk_bytes = 0, disk_seconds = 0;
 
  private:
   struct Entry {
     DModel m;
     std::vector<std::vector<double2>> host;   // per block (ham, then ops), when spilled
     bool spilled = false;
+    bool on_disk = false;                     // spilled, and its host copy moved to `file`
+    std::string file;
     long long bytes = 0;
     unsigned long long tick = 0;
   };
@@ -219,12 +232,18 @@ class ModelStore {
   void spill(Entry& e);
   void restore(Entry& e);
   void enforce(long long keep);
+  void to_disk(long long key, Entry& e);
+  void from_disk(Entry& e);
+  void enforce_host(long long keep);
   std::map<long long, Entry> map_;
   cudaStream_t st_ = nullptr;
   long long limit_ = -1;
   double default_frac_ = 0.45;
   long long resident_ = 0;
   unsigned long long clock_ = 0;
+  long long host_limit_ = -1;
+  std::string disk_dir_;
+  long long host_bytes_ = 0;   // bytes of the spilled models' host copies
 };
 
 // Pre-sliced operand views of a pair of split-precision lists (phase 1, phase 2).

@@ -5,6 +5,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstdlib>
+#include <cstdio>
 #include <cstring>
 #include <map>
 #include <mutex>
@@ -919,6 +920,7 @@ void ModelStore::spill(Entry& e) {
   for_blocks(e.m, [&](DBlock& b) { b.buf.reset(); });
   e.spilled = true;
   resident_ -= e.bytes;
+  host_bytes_ += e.bytes;
   spills++;
   moved_bytes += (double)e.bytes;
   moved_seconds += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
@@ -926,6 +928,7 @@ void ModelStore::spill(Entry& e) {
 
 void ModelStore::restore(Entry& e) {
   if (!e.spilled) return;
+  if (e.on_disk) from_disk(e);
   auto t0 = std::chrono::steady_clock::now();
   size_t k = 0;
   for_blocks(e.m, [&](DBlock& b) {
@@ -940,6 +943,7 @@ void ModelStore::restore(Entry& e) {
   e.host.shrink_to_fit();
   e.spilled = false;
   resident_ += e.bytes;
+  host_bytes_ -= e.bytes;
   restores++;
   moved_bytes += (double)e.bytes;
   moved_seconds += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
@@ -957,16 +961,24 @@ void ModelStore::enforce(long long keep) {
     if (!victim) break;
     spill(*victim);
   }
+  enforce_host(keep);
 }
 
 void ModelStore::put(int side, int len, const DModel& m) {
   const long long k = key(side, len);
   auto it = map_.find(k);
-  if (it != map_.end() && !it->second.spilled) resident_ -= it->second.bytes;
+  if (it != map_.end()) {
+    Entry& o = it->second;
+    if (!o.spilled) resident_ -= o.bytes;
+    else if (!o.on_disk) host_bytes_ -= o.bytes;
+    if (o.on_disk) std::remove(o.file.c_str());
+  }
   Entry& e = map_[k];
   e.m = m;
   e.host.clear();
   e.spilled = false;
+  e.on_disk = false;
+  e.file.clear();
   e.bytes = model_bytes(e.m);
   e.tick = ++clock_;
   resident_ += e.bytes;
@@ -985,6 +997,86 @@ DModel ModelStore::get(int side, int len) {
     enforce(k);
   }
   return e.m;
+}
+
+// host copies of the least recently used spilled models to files until the
+// spilled models' host bytes fit under the host limit
+void ModelStore::enforce_host(long long keep) {
+  if (host_limit_ < 0 || disk_dir_.empty()) return;
+  while (host_bytes_ > host_limit_) {
+    long long vk = 0;
+    Entry* victim = nullptr;
+    for (auto& kv : map_)
+      if (kv.first != keep && kv.second.spilled && !kv.second.on_disk && kv.second.bytes > 0 &&
+          (!victim || kv.second.tick < victim->tick)) {
+        victim = &kv.second;
+        vk = kv.first;
+      }
+    if (!victim) break;
+    to_disk(vk, *victim);
+  }
+}
+
+// one file per model: for every block, its element count (int64) and elements
+void ModelStore::to_disk(long long k, Entry& e) {
+  auto t0 = std::chrono::steady_clock::now();
+  e.file = disk_dir_ + "/tsc_model_" + std::to_string(k >> 32) + "_" + std::to_string(k & 0xffffffff) + "_" +
+           std::to_string(reinterpret_cast<uintptr_t>(this)) + ".bin";
+  std::FILE* f = std::fopen(e.file.c_str(), "wb");
+  if (!f) throw Error(-1, "model spill: cannot create " + e.file);
+  bool ok = true;
+  for (const auto& h : e.host) {
+    const long long n = (long long)h.size();
+    ok = ok && std::fwrite(&n, sizeof(n), 1, f) == 1;
+    if (n) ok = ok && std::fwrite(h.data(), sizeof(double2), (size_t)n, f) == (size_t)n;
+  }
+  ok = (std::fclose(f) == 0) && ok;
+  if (!ok) {
+    std::remove(e.file.c_str());
+    throw Error(-1, "model spill: cannot write " + e.file);
+  }
+  std::vector<std::vector<double2>>().swap(e.host);
+  e.on_disk = true;
+  host_bytes_ -= e.bytes;
+  disk_writes++;
+  disk_bytes += (double)e.bytes;
+  disk_seconds += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+}
+
+void ModelStore::from_disk(Entry& e) {
+  auto t0 = std::chrono::steady_clock::now();
+  std::FILE* f = std::fopen(e.file.c_str(), "rb");
+  if (!f) throw Error(-1, "model spill: cannot open " + e.file);
+  e.host.clear();
+  bool ok = true;
+  size_t nb = 0;
+  for_blocks(e.m, [&](DBlock&) { nb++; });
+  for (size_t i = 0; i < nb && ok; ++i) {
+    long long n = 0;
+    ok = std::fread(&n, sizeof(n), 1, f) == 1 && n >= 0;
+    e.host.emplace_back();
+    if (ok && n) {
+      e.host.back().resize((size_t)n);
+      ok = std::fread(e.host.back().data(), sizeof(double2), (size_t)n, f) == (size_t)n;
+    }
+  }
+  std::fclose(f);
+  if (!ok) throw Error(-1, "model spill: cannot read " + e.file);
+  std::remove(e.file.c_str());
+  e.file.clear();
+  e.on_disk = false;
+  host_bytes_ += e.bytes;
+  disk_reads++;
+  disk_bytes += (double)e.bytes;
+  disk_seconds += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+}
+
+void ModelStore::clear() {
+  for (auto& kv : map_)
+    if (kv.second.on_disk) std::remove(kv.second.file.c_str());
+  map_.clear();
+  resident_ = 0;
+  host_bytes_ = 0;
 }
 
 DBlock Engine::copy_block(const DBlock& b) {

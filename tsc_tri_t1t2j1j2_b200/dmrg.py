@@ -184,6 +184,20 @@ class Context:
         return {"spills": sp.value, "restores": rs.value, "bytes": by.value, "seconds": sec.value,
                 "resident_bytes": rb.value, "limit_bytes": lb.value}
 
+    def set_spill_directory(self, directory, host_bytes):
+        """Disk tier under the host spill: spilled models past host_bytes of host
+        memory go to files in `directory` (None: no disk tier)."""
+        d = os.fsencode(directory) if directory else None
+        self._check(self.L.tsc_set_spill_directory(self.h, d, int(host_bytes)))
+
+    def disk_spill_stats(self):
+        """{writes, reads, bytes, seconds, host_bytes} of the disk tier."""
+        w, r, hb = ctypes.c_longlong(), ctypes.c_longlong(), ctypes.c_longlong()
+        by, sec = ctypes.c_double(), ctypes.c_double()
+        self._check(self.L.tsc_disk_spill_stats(self.h, ctypes.byref(w), ctypes.byref(r), ctypes.byref(by),
+                                                ctypes.byref(sec), ctypes.byref(hb)))
+        return {"writes": w.value, "reads": r.value, "bytes": by.value, "seconds": sec.value, "host_bytes": hb.value}
+
     def blocksparse_set(self, problems):
         """Block-sparse batch (tsc_blocksparse_set): `problems` is a list of
         blocksparse.Problem; returns (psi length, algorithmic flops of one
