@@ -594,6 +594,7 @@ def fp64_hpsi(torch, dev, sb, model, steps, warmup, dist=None, clocks=None):
         ctx.hpsi_device(psi.data_ptr(), out.data_ptr())
         kms.append(ctx.hpsi_stats()["device_ms"])
     res = {"ms_total": ms, "ms_per_step": ms / steps, "ref_flops": st["ref_flops"], "exec_flops": st["exec_flops"],
+           "launches_per_step": st["launches"],
            "kernel_ms": float(np.mean(kms)), "schedule": schedule, "tune_table": tune_table,
            "clocks": sampler.summary() if sampler else None, "psi_amplitudes": n, "operator_elements": int(off)}
     return ctx, psi, out, res
@@ -662,11 +663,12 @@ def run_gpu(args):
                          "algorithmic_bytes_note": "every operator sub-block and psi element read once, every "
                                                    "output element written once, per H.psi",
                          "peak_source": "cuBLAS ZGEMM 4096^3 complex128 measured in this run (FP64 DMMA)",
-                         "kernel": "grouped_zgemm (2 launches per H.psi)",
+                         "kernel": "grouped_zgemm (2 launches per H.psi, + reduce_partials where a group's terms were split)",
                          "schedule": {"tile": r["schedule"][0], "waves": r["schedule"][1],
                                       "candidates_ms_per_gflop": {str(k): v for k, v in r["tune_table"].items()}}},
             "e2e": {"value": e2e, "unit": "TFLOP/s", "h2d_bytes_per_step": 16 * n, "d2h_bytes_per_step": 16 * n},
-            "gpu_launches": 2 * args.steps,
+            # the grouped GEMM of each phase plus the fixed-order reductions of split groups
+            "gpu_launches": r["launches_per_step"] * args.steps,
             "clocks": r["clocks"],
         }
         # side legs only at N = 1: under torchrun the other ranks wait at the closing
