@@ -39,6 +39,20 @@ def test_errors_are_status_codes_not_aborts():
     assert rc == -3
     assert b"cuda" in L.tsc_last_error(h).lower()
     assert L.tsc_superblock_dim(h) == -4
+    # entry points that need an engine report it as a status, never crash
+    d = (ctypes.c_double * 64)()
+    ii = (ctypes.c_int * 64)()
+    ll = ctypes.c_longlong()
+    assert L.tsc_measure_correlation(h, 1, 1, d, 16) == -4
+    assert L.tsc_measure_pair_correlation(h, 1, 16, 0, 1, ii, d, 8) == -4
+    assert L.tsc_set_lanczos_graph(h, 1) == -4
+    assert L.tsc_lanczos_graph_stats(h, ctypes.byref(ll), ctypes.byref(ll), None, 0) == -4
+    assert L.tsc_set_split_view_sharing(h, 1) == -4
+    assert L.tsc_set_split_finish_tolerance(h, 1.0) == -4
+    assert L.tsc_set_spill_directory(h, b"/tmp", 0) == -4
+    assert L.tsc_set_split_renormalization(h, 1) == -4
+    assert L.tsc_density_matrix(h, 0, d, 1, None, None, None, None) == -4
+    assert L.tsc_measure_correlation(None, 1, 1, d, 16) == -1
     assert L.tsc_destroy(h) == 0
     assert L.tsc_create(None, ctypes.byref(cfg)) == -1
     assert L.tsc_hpsi(None, None, None) == -1
